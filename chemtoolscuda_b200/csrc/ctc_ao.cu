@@ -1,0 +1,162 @@
+// ctc_ao.cu -- contracted Gaussian AOs and their first/second derivatives on points.
+//
+// Restates the reference's AO evaluation (src/evaluate_density.cu:25-393,
+// src/evaluate_gradient.cu:18-1127, src/evaluate_hessian.cu:17-1835) in one
+// generic form.  Every AO component of a segment is
+//     phi_j(r) = sum_t c_t x^a y^b z^c * R0(r^2),   R0 = sum_k coef_k exp(-alpha_k r^2)
+// (x, y, z relative to the shell centre; c_t from ctc_terms.inc).  With
+// R1 = sum_k alpha_k coef_k exp(..) and R2 = sum_k alpha_k^2 coef_k exp(..),
+//     d/dx   [x^a e] = a x^(a-1) R0 - 2 x^(a+1) R1
+//     d2/dx2 [x^a e] = a(a-1) x^(a-2) R0 - 2(2a+1) x^a R1 + 4 x^(a+2) R2
+//     d2/dxdy[x^a y^b e] = (a x^(a-1))(b y^(b-1)) R0 - 2(a x^(a-1) y^(b+1) + b x^(a+1) y^(b-1)) R1
+//                         + 4 x^(a+1) y^(b+1) R2
+// so one exponential per primitive serves every component and derivative.
+//
+// One thread evaluates one segment at a few points.  Segments are visited in
+// an order sorted by type and primitive count, so a warp runs one code path.
+// A segment whose centre is farther than its screening radius from the point
+// (every value and derivative below 1e-18) writes zeros without evaluating
+// exponentials.  Arithmetic is FP64 throughout.
+#include "ctc_internal.h"
+
+#include "ctc_terms.inc"
+
+namespace ctc {
+
+namespace {
+
+constexpr int kAoThreads = 128;
+
+template <int DERIV>
+__global__ void __launch_bounds__(kAoThreads)
+    ao_kernel(const DevSeg* __restrict__ segs, const int32_t* __restrict__ order, int nseg,
+              const double* __restrict__ alpha, const double* __restrict__ coef, PointSrc src,
+              int64_t n, int ppb, double* __restrict__ out, int nq_out, int64_t ld_point,
+              int64_t ld_q) {
+  constexpr int NQ = DERIV == 0 ? 1 : (DERIV == 1 ? 4 : 10);
+  int si = blockIdx.x * kAoThreads + threadIdx.x;
+  if (si >= nseg) return;
+  const DevSeg sg = segs[order[si]];
+  int nc;
+  switch (sg.type) {
+    case 0: nc = 1; break;
+    case 1: nc = 3; break;
+    case 2: nc = 6; break;
+    case 3: nc = 5; break;
+    case 4: nc = 10; break;
+    case 5: nc = 7; break;
+    case 6: nc = 15; break;
+    default: nc = 9; break;
+  }
+  int64_t p_begin = (int64_t)blockIdx.y * ppb;
+  int64_t p_end = min(p_begin + ppb, n);
+  for (int64_t p = p_begin; p < p_end; ++p) {
+    double px, py, pz;
+    point_of(src, p, px, py, pz);
+    double x = px - sg.cx, y = py - sg.cy, z = pz - sg.cz;
+    double r2 = x * x + y * y + z * z;
+    double* o = out + p * ld_point + sg.ao0;
+    if (r2 > sg.rcut2) {
+      for (int q = 0; q < nq_out; ++q)
+        for (int j = 0; j < nc; ++j) o[q * ld_q + j] = 0.0;
+      continue;
+    }
+    double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+    for (int k = 0; k < sg.nprim; ++k) {
+      double a = alpha[sg.prim0 + k];
+      double e = coef[sg.prim0 + k] * exp(-a * r2);
+      R0 += e;
+      if (DERIV >= 1) R1 += a * e;
+      if (DERIV >= 2) R2 += a * a * e;
+    }
+    // powers with two leading zeros: P[i] = x^(i-2), P[0] = P[1] = 0
+    double X[9], Y[9], Z[9];
+    X[0] = X[1] = Y[0] = Y[1] = Z[0] = Z[1] = 0.0;
+    X[2] = Y[2] = Z[2] = 1.0;
+#pragma unroll
+    for (int i = 3; i < 9; ++i) {
+      X[i] = X[i - 1] * x;
+      Y[i] = Y[i - 1] * y;
+      Z[i] = Z[i - 1] * z;
+    }
+    for (int j = 0; j < nc; ++j) {
+      double q[NQ];
+#pragma unroll
+      for (int i = 0; i < NQ; ++i) q[i] = 0.0;
+      const int tb = c_comp_off[sg.type][j], te = c_comp_off[sg.type][j + 1];
+      for (int t = tb; t < te; ++t) {
+        const Term T = c_terms[t];
+        const int a = T.a, b = T.b, c = T.z;
+        const double X0 = X[a + 2], Y0 = Y[b + 2], Z0 = Z[c + 2];
+        q[0] += T.c * X0 * Y0 * Z0 * R0;
+        if (DERIV >= 1) {
+          const double Xa = a * X[a + 1], Xb = X[a + 3];
+          const double Ya = b * Y[b + 1], Yb = Y[b + 3];
+          const double Za = c * Z[c + 1], Zb = Z[c + 3];
+          q[1] += T.c * Y0 * Z0 * (Xa * R0 - 2.0 * Xb * R1);
+          q[2] += T.c * X0 * Z0 * (Ya * R0 - 2.0 * Yb * R1);
+          q[3] += T.c * X0 * Y0 * (Za * R0 - 2.0 * Zb * R1);
+          if (DERIV >= 2) {
+            const double Xaa = a * (a - 1) * X[a], Xd = X[a + 4];
+            const double Yaa = b * (b - 1) * Y[b], Yd = Y[b + 4];
+            const double Zaa = c * (c - 1) * Z[c], Zd = Z[c + 4];
+            q[4] += T.c * Y0 * Z0 * (Xaa * R0 - 2.0 * (2 * a + 1) * X0 * R1 + 4.0 * Xd * R2);
+            q[5] += T.c * Z0 * (Xa * Ya * R0 - 2.0 * (Xa * Yb + Xb * Ya) * R1 + 4.0 * Xb * Yb * R2);
+            q[6] += T.c * Y0 * (Xa * Za * R0 - 2.0 * (Xa * Zb + Xb * Za) * R1 + 4.0 * Xb * Zb * R2);
+            q[7] += T.c * X0 * Z0 * (Yaa * R0 - 2.0 * (2 * b + 1) * Y0 * R1 + 4.0 * Yd * R2);
+            q[8] += T.c * X0 * (Ya * Za * R0 - 2.0 * (Ya * Zb + Yb * Za) * R1 + 4.0 * Yb * Zb * R2);
+            q[9] += T.c * X0 * Y0 * (Zaa * R0 - 2.0 * (2 * c + 1) * Z0 * R1 + 4.0 * Zd * R2);
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < NQ; ++i)
+        if (i < nq_out) o[i * ld_q + j] = q[i];
+    }
+  }
+}
+
+}  // namespace
+
+static int launch_ao_impl(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv,
+                          double* out, int nq_out, int64_t ld_point, int64_t ld_q, cudaStream_t st) {
+  if (n <= 0) return CTC_OK;
+  int ppb = 4;
+  int64_t gy = (n + ppb - 1) / ppb;
+  if (gy > 65535) {
+    ppb = (int)((n + 65534) / 65535);
+    gy = (n + ppb - 1) / ppb;
+  }
+  dim3 grid((mol->nseg + kAoThreads - 1) / kAoThreads, (unsigned)gy);
+  switch (deriv) {
+    case 0:
+      ao_kernel<0><<<grid, kAoThreads, 0, st>>>(mol->d_segs, mol->d_order, mol->nseg, mol->d_alpha,
+                                                mol->d_coef, src, n, ppb, out, nq_out, ld_point, ld_q);
+      break;
+    case 1:
+      ao_kernel<1><<<grid, kAoThreads, 0, st>>>(mol->d_segs, mol->d_order, mol->nseg, mol->d_alpha,
+                                                mol->d_coef, src, n, ppb, out, nq_out, ld_point, ld_q);
+      break;
+    default:
+      ao_kernel<2><<<grid, kAoThreads, 0, st>>>(mol->d_segs, mol->d_order, mol->nseg, mol->d_alpha,
+                                                mol->d_coef, src, n, ppb, out, nq_out, ld_point, ld_q);
+  }
+  CTC_CUDA_TRY(cudaGetLastError());
+  return CTC_OK;
+}
+
+// Local-descriptor layout: out[(p * nq_out + q) * ld + ao]; AO columns beyond
+// M (padding up to Mpad) are left untouched and must be zeroed by the caller.
+int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
+              int nq_out, int ld, cudaStream_t st) {
+  return launch_ao_impl(mol, src, n, deriv, out, nq_out, (int64_t)nq_out * ld, ld, st);
+}
+
+// Public layout (nq, n, M).
+int launch_ao_public(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv,
+                     double* out, cudaStream_t st) {
+  int nq = deriv == 0 ? 1 : (deriv == 1 ? 4 : 10);
+  return launch_ao_impl(mol, src, n, deriv, out, nq, mol->M, n * (int64_t)mol->M, st);
+}
+
+}  // namespace ctc

@@ -1,0 +1,233 @@
+// ctc_api.cu -- extern "C" entry points of include/chemtools_cuda.h.
+//
+// Device-pointer calls are stream-ordered and validate their arguments on the
+// host.  Host-pointer calls (the reference's own calling convention: host
+// arrays in, host vector out, e.g. src/evaluate_density.cu:663-673) stage
+// points and results through pinned buffers in slabs, so the copies of one
+// slab overlap the kernels of the next on two streams.
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "ctc_internal.h"
+
+using namespace ctc;
+
+namespace {
+
+bool any_output(const ctc_outputs* o) {
+  return o->rho || o->grad || o->hess || o->lap || o->tau_pd || o->tau_alpha || o->rdg ||
+         o->shannon || o->weizsacker || o->thomas_fermi || o->gge || o->general_ked;
+}
+
+ctc_params default_params(const ctc_params* p) {
+  if (p) return *p;
+  ctc_params d;
+  d.alpha = 0.0;
+  d.gge_a = 1.0 / 9.0;
+  d.gge_b = 1.0 / 6.0;
+  d.ked_a = 1.0;
+  return d;
+}
+
+// scalar widths of the output slots in doubles per point
+const int kWidth[12] = {1, 3, 9, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+
+double** slot(ctc_outputs* o, int i) {
+  double** s[12] = {&o->rho, &o->grad, &o->hess, &o->lap, &o->tau_pd, &o->tau_alpha,
+                    &o->rdg, &o->shannon, &o->weizsacker, &o->thomas_fermi, &o->gge,
+                    &o->general_ked};
+  return s[i];
+}
+
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~PinnedBuf() { if (p) cudaFreeHost(p); }
+  int ensure(size_t b) {
+    if (b <= bytes) return CTC_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMallocHost(&p, b) != cudaSuccess) return fail(CTC_ERR_NOMEM, "pinned host allocation failed");
+    bytes = b;
+    return CTC_OK;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int ctc_eval_local(ctc_molecule* mol, const double* d_points, int64_t n, int32_t precision,
+                   const ctc_params* params, const ctc_outputs* d_out, void* stream) {
+  if (!mol || !d_out) return fail(CTC_ERR_INVALID, "ctc_eval_local: null argument");
+  if (n < 0) return fail(CTC_ERR_INVALID, "ctc_eval_local: negative point count");
+  if (n > 0 && !d_points) return fail(CTC_ERR_INVALID, "ctc_eval_local: null points");
+  if (!any_output(d_out)) return CTC_OK;
+  PointSrc src{};
+  src.pts = d_points;
+  ctc_params prm = default_params(params);
+  return eval_local(mol, src, n, precision, &prm, d_out, (cudaStream_t)stream);
+}
+
+int ctc_eval_cubic(ctc_molecule* mol, const double* origin, const double* axes,
+                   const int32_t* shape, int32_t precision, const ctc_params* params,
+                   const ctc_outputs* d_out, void* stream) {
+  if (!mol || !origin || !axes || !shape || !d_out)
+    return fail(CTC_ERR_INVALID, "ctc_eval_cubic: null argument");
+  if (shape[0] < 0 || shape[1] < 0 || shape[2] < 0)
+    return fail(CTC_ERR_INVALID, "ctc_eval_cubic: negative shape");
+  if (!any_output(d_out)) return CTC_OK;
+  PointSrc src{};
+  src.cubic = 1;
+  for (int i = 0; i < 3; ++i) src.o[i] = origin[i];
+  for (int i = 0; i < 9; ++i) src.ax[i] = axes[i];
+  src.ny = shape[1];
+  src.nz = shape[2];
+  int64_t n = (int64_t)shape[0] * shape[1] * shape[2];
+  if (n == 0) return CTC_OK;
+  ctc_params prm = default_params(params);
+  return eval_local(mol, src, n, precision, &prm, d_out, (cudaStream_t)stream);
+}
+
+int ctc_eval_ao(ctc_molecule* mol, const double* d_points, int64_t n, int32_t deriv,
+                double* d_out, void* stream) {
+  if (!mol || !d_out || (n > 0 && !d_points)) return fail(CTC_ERR_INVALID, "ctc_eval_ao: null argument");
+  if (deriv < 0 || deriv > 2) return fail(CTC_ERR_INVALID, "ctc_eval_ao: deriv must be 0, 1 or 2");
+  if (n <= 0) return n < 0 ? fail(CTC_ERR_INVALID, "ctc_eval_ao: negative point count") : CTC_OK;
+  PointSrc src{};
+  src.pts = d_points;
+  return launch_ao_public(mol, src, n, deriv, d_out, (cudaStream_t)stream);
+}
+
+int ctc_eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, void* stream) {
+  if (!mol || !d_out || (n > 0 && !d_points)) return fail(CTC_ERR_INVALID, "ctc_eval_esp: null argument");
+  return eval_esp(mol, d_points, n, d_out, (cudaStream_t)stream);
+}
+
+int ctc_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const double* d_v_rho,
+                const double* d_v_grad, double* d_dLdD, double* d_dLdR, void* stream) {
+  if (!mol || (n > 0 && (!d_points || !d_v_rho)))
+    return fail(CTC_ERR_INVALID, "ctc_adjoint: null argument");
+  if (n < 0) return fail(CTC_ERR_INVALID, "ctc_adjoint: negative point count");
+  if (n == 0 || (!d_dLdD && !d_dLdR)) return CTC_OK;
+  return eval_adjoint(mol, d_points, n, d_v_rho, d_v_grad, d_dLdD, d_dLdR, (cudaStream_t)stream);
+}
+
+// Host-buffer variants: slabs of points go host -> device, through the
+// device path and back.  Kernels run on one compute stream (the molecule's
+// scratch is not shared across streams); the host->device copy of slab k+1
+// and the device->host copy of slab k-1 run on two copy streams while slab k
+// computes, ordered by events.
+int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, int32_t precision,
+                        const ctc_params* params, const ctc_outputs* h_out) {
+  if (!mol || !h_out || (n > 0 && !h_points)) return fail(CTC_ERR_INVALID, "ctc_eval_local_host: null argument");
+  if (n < 0) return fail(CTC_ERR_INVALID, "ctc_eval_local_host: negative point count");
+  if (n == 0 || !any_output(h_out)) return CTC_OK;
+  ctc_params prm = default_params(params);
+  int width = 3;
+  for (int i = 0; i < 12; ++i)
+    if (*slot(const_cast<ctc_outputs*>(h_out), i)) width += kWidth[i];
+  const int64_t slab = std::min<int64_t>(n, std::max<int64_t>(chunk_points(mol, plan_local(h_out).nq_ao), 1 << 18));
+  static thread_local PinnedBuf pin[2];
+  size_t slab_bytes = sizeof(double) * (size_t)slab * width;
+  cudaStream_t cs = 0, h2d = 0, d2h = 0;
+  cudaEvent_t ev_in[2] = {0, 0}, ev_comp[2] = {0, 0}, ev_out[2] = {0, 0};
+  double* dbuf[2] = {nullptr, nullptr};
+  int rc = CTC_OK;
+  auto cuda_ok = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && rc == CTC_OK) rc = fail(CTC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return rc == CTC_OK;
+  };
+  cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+  cuda_ok(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking), "stream");
+  cuda_ok(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking), "stream");
+  for (int b = 0; b < 2 && rc == CTC_OK; ++b) {
+    cuda_ok(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming), "event");
+    cuda_ok(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming), "event");
+    cuda_ok(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming), "event");
+    if (rc == CTC_OK) rc = pin[b].ensure(slab_bytes);
+    if (rc == CTC_OK && cudaMalloc((void**)&dbuf[b], slab_bytes) != cudaSuccess)
+      rc = fail(CTC_ERR_NOMEM, "ctc_eval_local_host: device staging allocation failed");
+  }
+  int64_t pending_off[2] = {-1, -1}, pending_n[2] = {0, 0};
+  auto drain = [&](int b) {
+    if (pending_off[b] < 0 || rc != CTC_OK) return;
+    if (!cuda_ok(cudaEventSynchronize(ev_out[b]), "ctc_eval_local_host: wait")) return;
+    const double* hb = (const double*)pin[b].p + 3 * (size_t)pending_n[b];
+    for (int i = 0; i < 12; ++i) {
+      double* dst = *slot(const_cast<ctc_outputs*>(h_out), i);
+      if (!dst) continue;
+      std::memcpy(dst + kWidth[i] * pending_off[b], hb, sizeof(double) * kWidth[i] * pending_n[b]);
+      hb += kWidth[i] * pending_n[b];
+    }
+    pending_off[b] = -1;
+  };
+  int b = 0;
+  for (int64_t off = 0; off < n && rc == CTC_OK; off += slab, b ^= 1) {
+    const int64_t m = std::min(slab, n - off);
+    drain(b);
+    if (rc != CTC_OK) break;
+    double* hp = (double*)pin[b].p;
+    double* dp = dbuf[b];
+    std::memcpy(hp, h_points + 3 * off, sizeof(double) * 3 * m);
+    if (!cuda_ok(cudaMemcpyAsync(dp, hp, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, h2d), "H2D") ||
+        !cuda_ok(cudaEventRecord(ev_in[b], h2d), "event") ||
+        !cuda_ok(cudaStreamWaitEvent(cs, ev_in[b], 0), "event"))
+      break;
+    ctc_outputs d{};
+    double* cur = dp + 3 * m;
+    for (int i = 0; i < 12; ++i) {
+      if (!*slot(const_cast<ctc_outputs*>(h_out), i)) continue;
+      *slot(&d, i) = cur;
+      cur += kWidth[i] * m;
+    }
+    PointSrc src{};
+    src.pts = dp;
+    rc = eval_local(mol, src, m, precision, &prm, &d, cs);
+    if (rc != CTC_OK) break;
+    if (!cuda_ok(cudaEventRecord(ev_comp[b], cs), "event") ||
+        !cuda_ok(cudaStreamWaitEvent(d2h, ev_comp[b], 0), "event") ||
+        !cuda_ok(cudaMemcpyAsync(hp + 3 * m, dp + 3 * m, sizeof(double) * (width - 3) * m,
+                                 cudaMemcpyDeviceToHost, d2h), "D2H") ||
+        !cuda_ok(cudaEventRecord(ev_out[b], d2h), "event"))
+      break;
+    pending_off[b] = off;
+    pending_n[b] = m;
+  }
+  drain(b);
+  drain(b ^ 1);
+  if (cs) cudaStreamSynchronize(cs);
+  if (h2d) cudaStreamSynchronize(h2d);
+  if (d2h) cudaStreamSynchronize(d2h);
+  for (int k = 0; k < 2; ++k) {
+    if (dbuf[k]) cudaFree(dbuf[k]);
+    if (ev_in[k]) cudaEventDestroy(ev_in[k]);
+    if (ev_comp[k]) cudaEventDestroy(ev_comp[k]);
+    if (ev_out[k]) cudaEventDestroy(ev_out[k]);
+  }
+  if (cs) cudaStreamDestroy(cs);
+  if (h2d) cudaStreamDestroy(h2d);
+  if (d2h) cudaStreamDestroy(d2h);
+  return rc;
+}
+
+int ctc_eval_esp_host(ctc_molecule* mol, const double* h_points, int64_t n, double* h_out) {
+  if (!mol || !h_out || (n > 0 && !h_points)) return fail(CTC_ERR_INVALID, "ctc_eval_esp_host: null argument");
+  if (n < 0) return fail(CTC_ERR_INVALID, "ctc_eval_esp_host: negative point count");
+  if (n == 0) return CTC_OK;
+  double* d = nullptr;
+  if (cudaMalloc((void**)&d, sizeof(double) * 4 * (size_t)n) != cudaSuccess)
+    return fail(CTC_ERR_NOMEM, "ctc_eval_esp_host: device allocation failed");
+  int rc = CTC_OK;
+  if (cudaMemcpy(d, h_points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = fail(CTC_ERR_CUDA, "ctc_eval_esp_host: H2D copy failed");
+  if (rc == CTC_OK) rc = eval_esp(mol, d, n, d + 3 * n, 0);
+  if (rc == CTC_OK && cudaMemcpy(h_out, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = fail(CTC_ERR_CUDA, "ctc_eval_esp_host: D2H copy failed");
+  cudaFree(d);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,312 @@
+// ctc_basis.cu -- molecule handle: basis tables, density matrix, scratch, errors.
+//
+// The reference packs its basis into a 60 KB __constant__ array before every
+// kernel launch, one constant-memory-sized chunk of shells at a time
+// (src/basis_to_gpu.cu:13-220).  Here a molecule handle owns its tables in
+// global memory, built once: one 56-byte record per segmented shell (centre,
+// screening radius, type, primitive range, first AO), primitive exponents and
+// coefficients with the radial normalisation N_l(a) = (2a/pi)^(3/4) (4a)^(l/2)
+// folded in (src/cuda_basis_utils.cu:7-109), and the AO -> atom map used by
+// the adjoint.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "ctc_internal.h"
+
+namespace ctc {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int type_of_angmom(int am) {
+  switch (am) {
+    case 0: return 0;
+    case 1: return 1;
+    case 2: return 2;
+    case -2: return 3;
+    case 3: return 4;
+    case -3: return 5;
+    case 4: return 6;
+    case -4: return 7;
+  }
+  return -1;
+}
+
+int ncomp_of_type(int t) {
+  static const int n[kNumTypes] = {1, 3, 6, 5, 10, 7, 15, 9};
+  return (t >= 0 && t < kNumTypes) ? n[t] : -1;
+}
+
+int l_of_type(int t) {
+  static const int l[kNumTypes] = {0, 1, 2, 2, 3, 3, 4, 4};
+  return (t >= 0 && t < kNumTypes) ? l[t] : -1;
+}
+
+int Scratch::ensure(size_t need, cudaStream_t st) {
+  if (need <= bytes) return CTC_OK;
+  if (p) {
+    cudaError_t e = cudaFreeAsync(p, st);
+    if (e != cudaSuccess) return fail(CTC_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(e));
+    p = nullptr;
+    bytes = 0;
+  }
+  size_t alloc = std::max(need, (size_t)1 << 20);
+  cudaError_t e = cudaMallocAsync(&p, alloc, st);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    return fail(CTC_ERR_NOMEM, std::string("scratch allocation of ") + std::to_string(alloc) +
+                                   " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes = alloc;
+  return CTC_OK;
+}
+
+void Scratch::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+int64_t chunk_points(const ctc_molecule* mol, int nq_ao) {
+  // AO buffer (nq * Mpad doubles per point) plus int8 planes; keep a chunk
+  // around 2 GB so that the working set stays bounded for any basis size.
+  size_t per_pt = (size_t)mol->Mpad * (8 * (size_t)nq_ao + 16);
+  int64_t n = (int64_t)((size_t)2 << 30) / (int64_t)per_pt;
+  n = std::max<int64_t>(n, 128);
+  n = std::min<int64_t>(n, 1 << 20);
+  return (n / 128) * 128;
+}
+
+int check_status(ctc_molecule* mol, cudaStream_t st, const char* what) {
+  int32_t h = 0;
+  CTC_CUDA_TRY(cudaMemcpyAsync(&h, mol->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CTC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h != 0) {
+    cudaMemsetAsync(mol->d_status, 0, sizeof(int32_t), st);
+    return fail(CTC_ERR_DEVICE, std::string(what) + ": kernel status " + std::to_string(h));
+  }
+  return CTC_OK;
+}
+
+// Radius beyond which |AO|, |grad AO| and |hess AO| of a segment stay below
+// eps for every component: a conservative bound using the largest polynomial
+// coefficient of the segment's type.
+static double screening_radius2(const std::vector<double>& a, const std::vector<double>& c, int l) {
+  const double eps = 1e-18;
+  const double tmax = 4.0;  // bound on |angular coefficients| (pure g peaks at ~3.4)
+  double rlast = 0.0;
+  for (double r = 0.05; r < 200.0; r += 0.05) {
+    double f = 0.0;
+    for (size_t k = 0; k < a.size(); ++k) {
+      double ar = a[k] * r;
+      double poly = std::pow(r, l) * (1.0 + l / std::max(r, 1e-3) + 2 * ar) *
+                    (1.0 + (l * l + l) / std::max(r * r, 1e-6) + 4 * ar * r + 4 * ar * ar + 2 * a[k]);
+      f += std::fabs(c[k]) * tmax * poly * std::exp(-a[k] * r * r);
+    }
+    if (f > eps) rlast = r;
+  }
+  double rc = rlast + 0.1;
+  return rc * rc;
+}
+
+}  // namespace ctc
+
+using namespace ctc;
+
+extern "C" {
+
+const char* ctc_last_error(void) { return g_last_error.c_str(); }
+
+const char* ctc_version(void) { return "chemtoolscuda_b200 0.1 (sm_100a)"; }
+
+int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xyz,
+                        const double* atom_charges, const double* D, int32_t nbasis,
+                        ctc_molecule** out) {
+  if (!b || !out || !D || (natom > 0 && (!atom_xyz || !atom_charges)))
+    return fail(CTC_ERR_INVALID, "ctc_molecule_create: null argument");
+  if (b->nshell <= 0 || !b->centers || !b->nprim || !b->nseg || !b->angmoms || !b->exps ||
+      !b->coeffs)
+    return fail(CTC_ERR_INVALID, "ctc_molecule_create: empty or incomplete basis");
+  *out = nullptr;
+  ctc_molecule* m = new ctc_molecule();
+  CTC_CUDA_TRY(cudaGetDevice(&m->device));
+  m->natom = natom;
+  m->atom_xyz.assign(atom_xyz, atom_xyz + 3 * (size_t)natom);
+  m->charges.assign(atom_charges, atom_charges + natom);
+  int ao = 0, ia = 0, ip = 0, ic = 0;
+  for (int s = 0; s < b->nshell; ++s) {
+    int K = b->nprim[s], S = b->nseg[s];
+    if (K <= 0 || S <= 0) {
+      delete m;
+      return fail(CTC_ERR_INVALID, "shell " + std::to_string(s) + ": nprim and nseg must be > 0");
+    }
+    int atom = b->shell_atom ? b->shell_atom[s] : -1;
+    if (!b->shell_atom) {
+      for (int a = 0; a < natom; ++a) {
+        double dx = b->centers[3 * s] - atom_xyz[3 * a], dy = b->centers[3 * s + 1] - atom_xyz[3 * a + 1],
+               dz = b->centers[3 * s + 2] - atom_xyz[3 * a + 2];
+        if (dx * dx + dy * dy + dz * dz < 1e-12) { atom = a; break; }
+      }
+    }
+    if (atom >= natom) {
+      delete m;
+      return fail(CTC_ERR_INVALID, "shell " + std::to_string(s) + ": atom index out of range");
+    }
+    for (int g = 0; g < S; ++g) {
+      int am = b->angmoms[ia + g];
+      int t = type_of_angmom(am);
+      if (t < 0) {
+        delete m;
+        return fail(CTC_ERR_INVALID, "shell " + std::to_string(s) + ": unsupported angular momentum " +
+                                         std::to_string(am) + " (supported: 0,1,+-2,+-3,+-4)");
+      }
+      DevSeg sg;
+      sg.cx = b->centers[3 * s];
+      sg.cy = b->centers[3 * s + 1];
+      sg.cz = b->centers[3 * s + 2];
+      sg.type = t;
+      sg.l = l_of_type(t);
+      sg.nprim = K;
+      sg.prim0 = (int)m->alpha.size();
+      sg.ao0 = ao;
+      sg.atom = atom;
+      std::vector<double> aa, cc;
+      for (int k = 0; k < K; ++k) {
+        double a = b->exps[ip + k];
+        if (!(a > 0.0)) {
+          delete m;
+          return fail(CTC_ERR_INVALID, "shell " + std::to_string(s) + ": exponents must be > 0");
+        }
+        double nrm = std::pow(2.0 * a / M_PI, 0.75) * std::pow(4.0 * a, 0.5 * sg.l);
+        aa.push_back(a);
+        cc.push_back(b->coeffs[ic + g * K + k] * nrm);
+      }
+      sg.rcut2 = screening_radius2(aa, cc, sg.l);
+      m->alpha.insert(m->alpha.end(), aa.begin(), aa.end());
+      m->coef.insert(m->coef.end(), cc.begin(), cc.end());
+      m->segs.push_back(sg);
+      for (int j = 0; j < ncomp_of_type(t); ++j) m->ao_atom.push_back(atom);
+      ao += ncomp_of_type(t);
+    }
+    ia += S;
+    ip += K;
+    ic += S * K;
+  }
+  if (ao != nbasis) {
+    delete m;
+    return fail(CTC_ERR_INVALID, "basis has " + std::to_string(ao) + " functions but D is " +
+                                     std::to_string(nbasis) + " x " + std::to_string(nbasis));
+  }
+  m->M = ao;
+  m->Mpad = (ao + 127) / 128 * 128;
+  m->nseg = (int)m->segs.size();
+  m->seg_order.resize(m->nseg);
+  for (int i = 0; i < m->nseg; ++i) m->seg_order[i] = i;
+  std::stable_sort(m->seg_order.begin(), m->seg_order.end(), [&](int x, int y) {
+    if (m->segs[x].type != m->segs[y].type) return m->segs[x].type < m->segs[y].type;
+    return m->segs[x].nprim < m->segs[y].nprim;
+  });
+  m->D.assign(D, D + (size_t)ao * ao);
+  m->ao_atom.resize(m->Mpad, -1);
+
+  size_t MM = (size_t)m->Mpad * m->Mpad;
+  std::vector<double> Dpad(MM, 0.0);
+  for (int i = 0; i < ao; ++i)
+    std::memcpy(&Dpad[(size_t)i * m->Mpad], D + (size_t)i * ao, sizeof(double) * ao);
+#define ALLOC_COPY(dst, src, count)                                                          \
+  do {                                                                                       \
+    cudaError_t _e = cudaMalloc((void**)&(dst), sizeof(*(dst)) * (count));                   \
+    if (_e == cudaSuccess)                                                                   \
+      _e = cudaMemcpy((dst), (src), sizeof(*(dst)) * (count), cudaMemcpyHostToDevice);       \
+    if (_e != cudaSuccess) {                                                                 \
+      ctc_molecule_destroy(m);                                                               \
+      return fail(CTC_ERR_NOMEM, std::string("device table upload: ") + cudaGetErrorString(_e)); \
+    }                                                                                        \
+  } while (0)
+  ALLOC_COPY(m->d_segs, m->segs.data(), m->segs.size());
+  ALLOC_COPY(m->d_alpha, m->alpha.data(), m->alpha.size());
+  ALLOC_COPY(m->d_coef, m->coef.data(), m->coef.size());
+  ALLOC_COPY(m->d_order, m->seg_order.data(), m->seg_order.size());
+  ALLOC_COPY(m->d_ao_atom, m->ao_atom.data(), m->ao_atom.size());
+  ALLOC_COPY(m->d_D, Dpad.data(), MM);
+#undef ALLOC_COPY
+  if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
+      cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
+    ctc_molecule_destroy(m);
+    return fail(CTC_ERR_NOMEM, "status word allocation failed");
+  }
+  *out = m;
+  return CTC_OK;
+}
+
+int ctc_molecule_destroy(ctc_molecule* m) {
+  if (!m) return CTC_OK;
+  cudaDeviceSynchronize();
+  destroy_esp(m);
+  cudaFree(m->d_segs);
+  cudaFree(m->d_alpha);
+  cudaFree(m->d_coef);
+  cudaFree(m->d_order);
+  cudaFree(m->d_ao_atom);
+  cudaFree(m->d_D);
+  cudaFree(m->d_Dsl);
+  cudaFree(m->d_Dscale);
+  cudaFree(m->d_status);
+  m->ws_ao.release();
+  m->ws_sl.release();
+  m->ws_part.release();
+  m->ws_misc.release();
+  delete m;
+  return CTC_OK;
+}
+
+int ctc_molecule_nbasis(const ctc_molecule* m) { return m ? m->M : fail(CTC_ERR_INVALID, "null molecule"); }
+int ctc_molecule_natom(const ctc_molecule* m) { return m ? m->natom : fail(CTC_ERR_INVALID, "null molecule"); }
+
+int ctc_molecule_set_density_matrix(ctc_molecule* m, const double* d_D, void* stream) {
+  if (!m || !d_D) return fail(CTC_ERR_INVALID, "set_density_matrix: null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  CTC_CUDA_TRY(cudaMemcpy2DAsync(m->d_D, sizeof(double) * m->Mpad, d_D, sizeof(double) * m->M,
+                                 sizeof(double) * m->M, m->M, cudaMemcpyDeviceToDevice, st));
+  CTC_CUDA_TRY(cudaMemcpyAsync(m->D.data(), d_D, sizeof(double) * m->M * m->M,
+                               cudaMemcpyDeviceToHost, st));
+  CTC_CUDA_TRY(cudaStreamSynchronize(st));
+  m->dsl_valid = false;
+  m->esp_valid = false;
+  return CTC_OK;
+}
+
+int ctc_molecule_set_coordinates(ctc_molecule* m, const double* xyz) {
+  if (!m || !xyz) return fail(CTC_ERR_INVALID, "set_coordinates: null argument");
+  for (auto& s : m->segs) {
+    if (s.atom < 0) continue;
+    s.cx = xyz[3 * s.atom];
+    s.cy = xyz[3 * s.atom + 1];
+    s.cz = xyz[3 * s.atom + 2];
+  }
+  m->atom_xyz.assign(xyz, xyz + 3 * (size_t)m->natom);
+  CTC_CUDA_TRY(cudaMemcpy(m->d_segs, m->segs.data(), sizeof(DevSeg) * m->segs.size(),
+                          cudaMemcpyHostToDevice));
+  m->esp_valid = false;
+  return CTC_OK;
+}
+
+int ctc_molecule_prepare(ctc_molecule* m, int32_t precision) {
+  if (!m) return fail(CTC_ERR_INVALID, "prepare: null molecule");
+  if (precision == CTC_PREC_TC_SPLIT) return prepare_tc(m, 0);
+  if (precision != CTC_PREC_FP64) return fail(CTC_ERR_INVALID, "prepare: unknown precision");
+  return CTC_OK;
+}
+
+}  // extern "C"

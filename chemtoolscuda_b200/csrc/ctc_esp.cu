@@ -1,0 +1,443 @@
+// ctc_esp.cu -- molecular electrostatic potential from Hermite pair densities.
+//
+// The reference builds all M(M+1)/2 point-charge integrals V_{mu nu}(C) per
+// point with the McMurchie-Davidson E and R recursions (Helgaker 9.5.6-7,
+// 9.9.18-20; include/integral_coeffs.cuh:17-238, src/evaluate_electrostatic.cu:
+// 16-10158) and then contracts them with D in a serial host loop of cublasDtpttr,
+// cublasDsymm, a Hadamard product and thrust::reduce per point
+// (src/evaluate_electrostatic.cu:10319-10344).  Since
+//     sum_{mu nu} D_{mu nu} V_{mu nu}(C)
+//        = sum_{pairs ab} (2 pi / p) sum_{tuv} h^{ab}_{tuv} R_{tuv}(p, P - C),
+//     h^{ab}_{tuv} = sum_{mu in a, nu in b} D_{mu nu} c_mu c_nu E^x_t E^y_u E^z_v
+// depends on the point only through R, the Hermite densities h are built once
+// per molecule (host, all cores) and each point costs one Boys evaluation and
+// one R recursion per significant primitive pair -- no integral matrix.
+//
+// Boys function F_n(T) (FP64): for T < 40 a 7-term Taylor expansion about the
+// nearest point of a 0.05-spaced table gives F_L, and F_{n-1} = (2T F_n +
+// e^{-T})/(2n-1) (downward recursion, stable) gives the rest; for T >= 40,
+// F_0 = sqrt(pi/T)/2 and upward recursion (stable there).  The table is built
+// at set-up from the series F_m(T) = e^{-T} sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
+// (The reference uses forward recursion from erf, include/boys_functions.cuh:13-31,
+// which loses digits at small T and divides by zero at T = 0.)
+//
+// V(C) = sum_A Z_A / |C - R_A| - electronic part (src/evaluate_electrostatic.cu:10357-10369).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "ctc_internal.h"
+
+#define CTC_TERMS_HOST
+#include "ctc_terms.inc"
+#undef CTC_TERMS_HOST
+
+namespace ctc {
+
+namespace {
+
+constexpr int kLmax = 8;                 // g x g
+constexpr int kTaylor = 7;               // terms of the Taylor expansion
+constexpr int kNF = kLmax + kTaylor;     // orders stored per table point
+constexpr double kTstep = 0.05;
+constexpr double kTmax = 40.0;
+constexpr int kNT = (int)(kTmax / kTstep) + 2;
+constexpr double kPi = 3.14159265358979323846;
+
+__host__ __device__ constexpr int ntuv(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+// index of (t,u,v): totals ascending; within a total s, t descending then u descending
+__host__ __device__ constexpr int tuv_index(int t, int u, int v) {
+  int s = t + u + v;
+  int base = s * (s + 1) * (s + 2) / 6;
+  int before = 0;
+  for (int tt = s; tt > t; --tt) before += s - tt + 1;
+  return base + before + (s - t - u);
+}
+
+struct EspPair {
+  double Px, Py, Pz, p, pref;  // pref = 2 pi / p
+};
+struct EspBatch {
+  int32_t b0, b1;   // pairs [b0, b1)
+  int32_t h0;       // first Hermite coefficient
+  int32_t L;
+};
+
+double boys_series(int m, double T) {
+  double term = 1.0 / (2 * m + 1), sum = term;
+  for (int i = 1; i < 1000; ++i) {
+    term *= 2.0 * T / (2 * m + 2 * i + 1);
+    sum += term;
+    if (term < 1e-18 * sum) break;
+  }
+  return std::exp(-T) * sum;
+}
+
+}  // namespace
+
+struct EspTables {
+  double* d_boys = nullptr;
+  EspPair* d_pairs = nullptr;
+  double* d_h = nullptr;
+  EspBatch* d_batches = nullptr;
+  double* d_atoms = nullptr;  // x y z Z per atom
+  int npairs = 0, nbatch = 0, natom = 0;
+  size_t nh = 0;
+};
+
+namespace {
+
+// ------------------------------------------------------------------ device side
+template <int L>
+__device__ __forceinline__ void boys(double T, const double* __restrict__ tab, double* F) {
+  const double e = exp(-T);
+  if (T < kTmax) {
+    const int i = __double2int_rn(T * (1.0 / kTstep));
+    const double d = i * kTstep - T;  // -(T - T_i)
+    const double* row = tab + i * kNF + L;
+    double fl = row[kTaylor - 1];
+#pragma unroll
+    for (int k = kTaylor - 2; k >= 0; --k) fl = row[k] + fl * d / (double)(k + 1);
+    F[L] = fl;
+#pragma unroll
+    for (int n = L; n > 0; --n) F[n - 1] = (2.0 * T * F[n] + e) / (2 * n - 1);
+  } else {
+    F[0] = 0.5 * sqrt(kPi / T);
+    const double inv2T = 0.5 / T;
+#pragma unroll
+    for (int n = 1; n <= L; ++n) F[n] = ((2 * n - 1) * F[n - 1] - e) * inv2T;
+  }
+}
+
+// R^0_{tuv}(p, X, Y, Z) for t+u+v <= L, in place from level L down to 0.
+template <int L>
+__device__ __forceinline__ void hermite_r(double p, double X, double Y, double Z, const double* F,
+                                          double* R) {
+  double m2p[L + 1];
+  m2p[0] = 1.0;
+#pragma unroll
+  for (int n = 1; n <= L; ++n) m2p[n] = m2p[n - 1] * (-2.0 * p);
+  R[0] = m2p[L] * F[L];
+#pragma unroll
+  for (int n = L - 1; n >= 0; --n) {
+    // level n: totals L-n down to 1 from level n+1, then total 0
+#pragma unroll
+    for (int s = L - n; s >= 1; --s) {
+#pragma unroll
+      for (int t = s; t >= 0; --t) {
+#pragma unroll
+        for (int u = s - t; u >= 0; --u) {
+          const int v = s - t - u;
+          double r;
+          if (t > 0) {
+            r = X * R[tuv_index(t - 1, u, v)];
+            if (t > 1) r += (t - 1) * R[tuv_index(t - 2, u, v)];
+          } else if (u > 0) {
+            r = Y * R[tuv_index(t, u - 1, v)];
+            if (u > 1) r += (u - 1) * R[tuv_index(t, u - 2, v)];
+          } else {
+            r = Z * R[tuv_index(t, u, v - 1)];
+            if (v > 1) r += (v - 1) * R[tuv_index(t, u, v - 2)];
+          }
+          R[tuv_index(t, u, v)] = r;
+        }
+      }
+    }
+    R[0] = m2p[n] * F[n];
+  }
+}
+
+template <int L>
+__device__ __forceinline__ double esp_batch(const EspPair* sp, const double* sh, int np, double cx,
+                                            double cy, double cz, const double* __restrict__ tab) {
+  constexpr int NT = ntuv(L);
+  double acc = 0.0;
+  for (int i = 0; i < np; ++i) {
+    const EspPair q = sp[i];
+    const double X = q.Px - cx, Y = q.Py - cy, Z = q.Pz - cz;
+    const double T = q.p * (X * X + Y * Y + Z * Z);
+    double F[L + 1];
+    boys<L>(T, tab, F);
+    double R[NT];
+    hermite_r<L>(q.p, X, Y, Z, F, R);
+    const double* h = sh + i * NT;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) s += h[k] * R[k];
+    acc += q.pref * s;
+  }
+  return acc;
+}
+
+constexpr int kEspThreads = 128;
+constexpr int kBatchPairs = 64;
+constexpr int kBatchH = 4096;
+
+__global__ void __launch_bounds__(kEspThreads)
+    esp_kernel(const EspPair* __restrict__ pairs, const double* __restrict__ hbuf,
+               const EspBatch* __restrict__ batches, int nbatch, const double* __restrict__ tab,
+               const double* __restrict__ atoms, int natom, const double* __restrict__ pts,
+               int64_t n, double* __restrict__ out) {
+  __shared__ EspPair sp[kBatchPairs];
+  __shared__ double sh[kBatchH];
+  const int64_t ip = (int64_t)blockIdx.x * kEspThreads + threadIdx.x;
+  const bool live = ip < n;
+  double cx = 0, cy = 0, cz = 0;
+  if (live) {
+    cx = pts[3 * ip];
+    cy = pts[3 * ip + 1];
+    cz = pts[3 * ip + 2];
+  }
+  double elec = 0.0;
+  for (int b = 0; b < nbatch; ++b) {
+    const EspBatch bt = batches[b];
+    const int np = bt.b1 - bt.b0;
+    const int nh = np * ntuv(bt.L);
+    __syncthreads();
+    for (int i = threadIdx.x; i < np; i += kEspThreads) sp[i] = pairs[bt.b0 + i];
+    for (int i = threadIdx.x; i < nh; i += kEspThreads) sh[i] = hbuf[bt.h0 + i];
+    __syncthreads();
+    if (!live) continue;
+    switch (bt.L) {
+      case 0: elec += esp_batch<0>(sp, sh, np, cx, cy, cz, tab); break;
+      case 1: elec += esp_batch<1>(sp, sh, np, cx, cy, cz, tab); break;
+      case 2: elec += esp_batch<2>(sp, sh, np, cx, cy, cz, tab); break;
+      case 3: elec += esp_batch<3>(sp, sh, np, cx, cy, cz, tab); break;
+      case 4: elec += esp_batch<4>(sp, sh, np, cx, cy, cz, tab); break;
+      case 5: elec += esp_batch<5>(sp, sh, np, cx, cy, cz, tab); break;
+      case 6: elec += esp_batch<6>(sp, sh, np, cx, cy, cz, tab); break;
+      case 7: elec += esp_batch<7>(sp, sh, np, cx, cy, cz, tab); break;
+      default: elec += esp_batch<8>(sp, sh, np, cx, cy, cz, tab); break;
+    }
+  }
+  if (!live) return;
+  double nuc = 0.0;
+  for (int a = 0; a < natom; ++a) {
+    const double dx = cx - atoms[4 * a], dy = cy - atoms[4 * a + 1], dz = cz - atoms[4 * a + 2];
+    nuc += atoms[4 * a + 3] / sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  out[ip] = nuc - elec;
+}
+
+// ------------------------------------------------------------------ host side
+void hermite_e(int la, int lb, double a, double b, double XAB, std::vector<double>& E) {
+  const int L = la + lb;
+  const double p = a + b, mu = a * b / p;
+  const double XPA = -(b / p) * XAB, XPB = (a / p) * XAB;
+  E.assign((size_t)(la + 1) * (lb + 1) * (L + 1), 0.0);
+  auto at = [&](int i, int j, int t) -> double& { return E[((size_t)i * (lb + 1) + j) * (L + 1) + t]; };
+  at(0, 0, 0) = std::exp(-mu * XAB * XAB);
+  for (int i = 0; i <= la; ++i)
+    for (int j = 0; j <= lb; ++j) {
+      if (i == 0 && j == 0) continue;
+      for (int t = 0; t <= i + j; ++t) {
+        if (j == 0) {
+          double em = t >= 1 ? at(i - 1, 0, t - 1) : 0.0;
+          double e0 = t <= i - 1 ? at(i - 1, 0, t) : 0.0;
+          double ep = t + 1 <= i - 1 ? at(i - 1, 0, t + 1) : 0.0;
+          at(i, j, t) = em / (2 * p) + XPA * e0 + (t + 1) * ep;
+        } else {
+          double em = t >= 1 ? at(i, j - 1, t - 1) : 0.0;
+          double e0 = t <= i + j - 1 ? at(i, j - 1, t) : 0.0;
+          double ep = t + 1 <= i + j - 1 ? at(i, j - 1, t + 1) : 0.0;
+          at(i, j, t) = em / (2 * p) + XPB * e0 + (t + 1) * ep;
+        }
+      }
+    }
+}
+
+struct Mono { int a, b, c; };
+
+// Cartesian monomials of degree l and the component -> monomial coefficient matrix.
+void seg_monomials(int type, std::vector<Mono>& monos, std::vector<double>& Tm /*ncomp x nmono*/) {
+  const int l = l_of_type(type), nc = ncomp_of_type(type);
+  monos.clear();
+  for (int a = l; a >= 0; --a)
+    for (int b = l - a; b >= 0; --b) monos.push_back({a, b, l - a - b});
+  Tm.assign((size_t)nc * monos.size(), 0.0);
+  for (int j = 0; j < nc; ++j)
+    for (int t = h_comp_off[type][j]; t < h_comp_off[type][j + 1]; ++t) {
+      const Term& T = h_terms[t];
+      for (size_t m = 0; m < monos.size(); ++m)
+        if (monos[m].a == T.a && monos[m].b == T.b && monos[m].c == T.z) Tm[j * monos.size() + m] += T.c;
+    }
+}
+
+struct PairOut {
+  int L;
+  EspPair pr;
+  std::vector<double> h;
+};
+
+}  // namespace
+
+void destroy_esp(ctc_molecule* mol) {
+  if (!mol->esp) return;
+  cudaFree(mol->esp->d_boys);
+  cudaFree(mol->esp->d_pairs);
+  cudaFree(mol->esp->d_h);
+  cudaFree(mol->esp->d_batches);
+  cudaFree(mol->esp->d_atoms);
+  delete mol->esp;
+  mol->esp = nullptr;
+  mol->esp_valid = false;
+}
+
+static int build_esp(ctc_molecule* mol) {
+  destroy_esp(mol);
+  for (const DevSeg& s : mol->segs)
+    if (s.l > 4) return fail(CTC_ERR_UNSUPPORTED, "ESP: angular momentum above g");
+  const int nseg = mol->nseg, M = mol->M;
+  // per-segment monomial data
+  std::vector<std::vector<Mono>> monos(nseg);
+  std::vector<std::vector<double>> Tm(nseg);
+  for (int s = 0; s < nseg; ++s) seg_monomials(mol->segs[s].type, monos[s], Tm[s]);
+  const double eps = 1e-17;
+  unsigned nthr = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  std::vector<std::vector<PairOut>> outs(nthr);
+  auto worker = [&](unsigned tid) {
+    std::vector<double> Ex, Ey, Ez, Dc;
+    for (int I = (int)tid; I < nseg; I += (int)nthr) {
+      const DevSeg& A = mol->segs[I];
+      const int nA = ncomp_of_type(A.type), mA = (int)monos[I].size();
+      for (int J = I; J < nseg; ++J) {
+        const DevSeg& B = mol->segs[J];
+        const int nB = ncomp_of_type(B.type), mB = (int)monos[J].size();
+        const double fac = (I == J) ? 1.0 : 2.0;
+        // Cartesian-monomial density Dc = Tm_A^T D_AB Tm_B
+        Dc.assign((size_t)mA * mB, 0.0);
+        double dmax = 0.0;
+        for (int i = 0; i < nA; ++i)
+          for (int j = 0; j < nB; ++j) {
+            const double d = mol->D[(size_t)(A.ao0 + i) * M + (B.ao0 + j)];
+            if (d == 0.0) continue;
+            for (int ma = 0; ma < mA; ++ma) {
+              const double ta = Tm[I][(size_t)i * mA + ma];
+              if (ta == 0.0) continue;
+              for (int mb = 0; mb < mB; ++mb) Dc[(size_t)ma * mB + mb] += d * ta * Tm[J][(size_t)j * mB + mb];
+            }
+          }
+        for (double v : Dc) dmax = std::max(dmax, std::fabs(v));
+        if (dmax == 0.0) continue;
+        const int L = A.l + B.l, NT = ntuv(L);
+        const double XAB = A.cx - B.cx, YAB = A.cy - B.cy, ZAB = A.cz - B.cz;
+        const double R2 = XAB * XAB + YAB * YAB + ZAB * ZAB;
+        for (int ka = 0; ka < A.nprim; ++ka) {
+          const double a = mol->alpha[A.prim0 + ka], ca = mol->coef[A.prim0 + ka];
+          for (int kb = 0; kb < B.nprim; ++kb) {
+            const double b = mol->alpha[B.prim0 + kb], cb = mol->coef[B.prim0 + kb];
+            const double p = a + b, mu = a * b / p;
+            const double K = std::exp(-mu * R2);
+            const double pref = 2.0 * kPi / p;
+            const double scale = fac * ca * cb;
+            // bound on |h| * |R| (|R_tuv| <= (2p)^(s/2) * s!! F-like factors)
+            const double bound = std::fabs(scale) * K * dmax * pref * mA * mB *
+                                 std::pow(1.0 + 2.0 * p, 0.5 * L) * std::pow(2.0, L);
+            if (bound < eps) continue;
+            hermite_e(A.l, B.l, a, b, XAB, Ex);
+            hermite_e(A.l, B.l, a, b, YAB, Ey);
+            hermite_e(A.l, B.l, a, b, ZAB, Ez);
+            PairOut po;
+            po.L = L;
+            po.pr = {(a * A.cx + b * B.cx) / p, (a * A.cy + b * B.cy) / p, (a * A.cz + b * B.cz) / p, p, pref};
+            po.h.assign(NT, 0.0);
+            const int LB1 = B.l + 1, L1 = L + 1;
+            for (int ma = 0; ma < mA; ++ma) {
+              const Mono& u = monos[I][ma];
+              for (int mb = 0; mb < mB; ++mb) {
+                const double dc = Dc[(size_t)ma * mB + mb] * scale;
+                if (dc == 0.0) continue;
+                const Mono& w = monos[J][mb];
+                for (int t = 0; t <= u.a + w.a; ++t) {
+                  const double ex = Ex[((size_t)u.a * LB1 + w.a) * L1 + t] * dc;
+                  for (int uu = 0; uu <= u.b + w.b; ++uu) {
+                    const double exy = ex * Ey[((size_t)u.b * LB1 + w.b) * L1 + uu];
+                    for (int v = 0; v <= u.c + w.c; ++v)
+                      po.h[tuv_index(t, uu, v)] += exy * Ez[((size_t)u.c * LB1 + w.c) * L1 + v];
+                  }
+                }
+              }
+            }
+            outs[tid].push_back(std::move(po));
+          }
+        }
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nthr; ++t) th.emplace_back(worker, t);
+  for (auto& t : th) t.join();
+  // gather, sorted by L, into batches of equal L
+  std::vector<EspPair> pairs;
+  std::vector<double> hv;
+  std::vector<EspBatch> batches;
+  for (int L = 0; L <= kLmax; ++L) {
+    const int NT = ntuv(L);
+    const int per = std::max(1, std::min(kBatchPairs, kBatchH / NT));
+    int in_batch = 0;
+    for (auto& o : outs)
+      for (auto& po : o) {
+        if (po.L != L) continue;
+        if (in_batch == 0) batches.push_back({(int32_t)pairs.size(), (int32_t)pairs.size(), (int32_t)hv.size(), L});
+        pairs.push_back(po.pr);
+        hv.insert(hv.end(), po.h.begin(), po.h.end());
+        batches.back().b1 = (int32_t)pairs.size();
+        if (++in_batch == per) in_batch = 0;
+      }
+  }
+  if (hv.size() > (size_t)INT32_MAX) return fail(CTC_ERR_UNSUPPORTED, "ESP: too many pair coefficients");
+  // Boys table
+  std::vector<double> tab((size_t)kNT * kNF);
+  for (int i = 0; i < kNT; ++i)
+    for (int m = 0; m < kNF; ++m) tab[(size_t)i * kNF + m] = boys_series(m, i * kTstep);
+  std::vector<double> atoms(4 * (size_t)std::max(mol->natom, 1));
+  for (int a = 0; a < mol->natom; ++a) {
+    atoms[4 * a] = mol->atom_xyz[3 * a];
+    atoms[4 * a + 1] = mol->atom_xyz[3 * a + 1];
+    atoms[4 * a + 2] = mol->atom_xyz[3 * a + 2];
+    atoms[4 * a + 3] = mol->charges[a];
+  }
+  EspTables* e = new EspTables();
+  mol->esp = e;
+  e->npairs = (int)pairs.size();
+  e->nbatch = (int)batches.size();
+  e->natom = mol->natom;
+  e->nh = hv.size();
+  auto up = [&](void** dst, const void* src, size_t bytes) -> int {
+    if (bytes == 0) bytes = 8;
+    CTC_CUDA_TRY(cudaMalloc(dst, bytes));
+    if (src) CTC_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return CTC_OK;
+  };
+  int rc;
+  if ((rc = up((void**)&e->d_boys, tab.data(), tab.size() * sizeof(double))) ||
+      (rc = up((void**)&e->d_pairs, pairs.empty() ? nullptr : pairs.data(), pairs.size() * sizeof(EspPair))) ||
+      (rc = up((void**)&e->d_h, hv.empty() ? nullptr : hv.data(), hv.size() * sizeof(double))) ||
+      (rc = up((void**)&e->d_batches, batches.empty() ? nullptr : batches.data(), batches.size() * sizeof(EspBatch))) ||
+      (rc = up((void**)&e->d_atoms, atoms.data(), atoms.size() * sizeof(double)))) {
+    destroy_esp(mol);
+    return rc;
+  }
+  mol->esp_valid = true;
+  return CTC_OK;
+}
+
+int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, cudaStream_t st) {
+  if (n < 0) return fail(CTC_ERR_INVALID, "eval_esp: negative point count");
+  if (n == 0) return CTC_OK;
+  if (!mol->esp_valid) {
+    int rc = build_esp(mol);
+    if (rc != CTC_OK) return rc;
+  }
+  const EspTables* e = mol->esp;
+  const int64_t grid = (n + kEspThreads - 1) / kEspThreads;
+  esp_kernel<<<(unsigned)grid, kEspThreads, 0, st>>>(e->d_pairs, e->d_h, e->d_batches, e->nbatch,
+                                                      e->d_boys, e->d_atoms, e->natom, d_points, n,
+                                                      d_out);
+  CTC_CUDA_TRY(cudaGetLastError());
+  return CTC_OK;
+}
+
+}  // namespace ctc

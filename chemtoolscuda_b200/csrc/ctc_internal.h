@@ -1,0 +1,164 @@
+// ctc_internal.h -- shared declarations of the B200 grid-evaluation library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/chemtools_cuda.h"
+
+namespace ctc {
+
+// --------------------------------------------------------------------------- error handling
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+
+#define CTC_CUDA_TRY(expr)                                                               \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return ::ctc::fail(CTC_ERR_CUDA, std::string(#expr " -> ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+// --------------------------------------------------------------------------- basis tables
+// Segment types: fchk angular-momentum code -> table index.
+//   0 s, 1 p, 2 d (6), -2 d (5), 3 f (10), -3 f (7), 4 g (15), -4 g (9)
+constexpr int kNumTypes = 8;
+int type_of_angmom(int angmom);          // -1 when unknown
+int ncomp_of_type(int type);
+int l_of_type(int type);
+
+// One segmented shell as the kernels see it (64 bytes).
+struct DevSeg {
+  double cx, cy, cz;
+  double rcut2;     // squared radius beyond which every AO (and derivative) is < 1e-18
+  int32_t type;     // 0..7
+  int32_t l;
+  int32_t nprim;
+  int32_t prim0;    // first primitive in the primitive arrays
+  int32_t ao0;      // first AO index
+  int32_t atom;     // owning atom or -1
+};
+static_assert(sizeof(DevSeg) == 56 || sizeof(DevSeg) == 64, "DevSeg layout");
+
+// Polynomial term of one AO component: coef * x^a y^b z^c (angular normalisation folded in).
+struct Term {
+  double c;
+  int8_t a, b, z, pad;
+};
+
+// Where the point coordinates of a launch come from.
+struct PointSrc {
+  const double* pts;   // row-major (N,3) when not cubic
+  double o[3];         // cubic origin
+  double ax[9];        // cubic axes, row i = axis i
+  int32_t ny, nz;      // cubic shape (x extent implied)
+  int32_t cubic;
+  int64_t offset;      // global index of the first point of this launch
+};
+
+__host__ __device__ inline void point_of(const PointSrc& s, int64_t i, double& x, double& y,
+                                         double& z) {
+  int64_t g = s.offset + i;
+  if (s.cubic) {
+    int64_t k = g % s.nz;
+    int64_t j = (g / s.nz) % s.ny;
+    int64_t ii = g / ((int64_t)s.nz * s.ny);
+    double fi = (double)ii, fj = (double)j, fk = (double)k;
+    x = s.o[0] + fi * s.ax[0] + fj * s.ax[3] + fk * s.ax[6];
+    y = s.o[1] + fi * s.ax[1] + fj * s.ax[4] + fk * s.ax[7];
+    z = s.o[2] + fi * s.ax[2] + fj * s.ax[5] + fk * s.ax[8];
+  } else {
+    x = s.pts[3 * g];
+    y = s.pts[3 * g + 1];
+    z = s.pts[3 * g + 2];
+  }
+}
+
+// Device scratch owned by a molecule; grows on demand, released stream-ordered.
+struct Scratch {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need, cudaStream_t st);
+  void release();
+};
+
+// ESP pair data built once per molecule (see ctc_esp.cu).
+struct EspTables;
+
+}  // namespace ctc
+
+struct ctc_molecule {
+  int device = 0;
+  int natom = 0, M = 0, Mpad = 0, nseg = 0;
+  std::vector<ctc::DevSeg> segs;             // host copy
+  std::vector<double> alpha, coef;           // host copies (coef includes N_l(alpha))
+  std::vector<int32_t> seg_order;            // segments sorted by type, nprim
+  std::vector<double> atom_xyz, charges;
+  std::vector<double> D;                     // host copy, M x M
+  std::vector<int32_t> ao_atom;              // AO -> atom
+  // device tables
+  ctc::DevSeg* d_segs = nullptr;
+  double* d_alpha = nullptr;
+  double* d_coef = nullptr;
+  int32_t* d_order = nullptr;
+  int32_t* d_ao_atom = nullptr;
+  double* d_D = nullptr;                     // Mpad x Mpad, zero padded
+  // split-precision copy of D (4 int8 byte planes, row scales)
+  int8_t* d_Dsl = nullptr;
+  double* d_Dscale = nullptr;
+  bool dsl_valid = false;
+  // per-call status word written by kernels
+  int32_t* d_status = nullptr;
+  // scratch
+  ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc;
+  ctc::EspTables* esp = nullptr;
+  bool esp_valid = false;
+};
+
+namespace ctc {
+
+// ---- kernels / launchers (ctc_ao.cu) ----
+int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
+              int nq_out, int ld, cudaStream_t st);
+// AO output in (nq, n, M) layout for ctc_eval_ao.
+int launch_ao_public(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv,
+                     double* out, cudaStream_t st);
+
+// ---- local descriptors (ctc_local.cu) ----
+struct LocalPlan {
+  int nq_ao;    // AO quantities produced per point (1, 4, 10)
+  int nqa;      // GEMM row quantities (1: Phi only, 4: Phi and grad Phi)
+  int deriv;    // AO derivative order
+};
+LocalPlan plan_local(const ctc_outputs* o);
+int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
+               const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
+
+// ---- tensor-core split path (ctc_tc.cu) ----
+int prepare_tc(ctc_molecule* mol, cudaStream_t st);
+int tc_local_chunk(ctc_molecule* mol, const LocalPlan& plan, const double* ao, int64_t n,
+                   int64_t out_offset, const ctc_params* prm, const ctc_outputs* out,
+                   cudaStream_t st);
+
+// ---- FP64 path (ctc_local.cu) ----
+int fp64_local_chunk(ctc_molecule* mol, const LocalPlan& plan, const double* ao, int64_t n,
+                     int64_t out_offset, const ctc_params* prm, const ctc_outputs* out,
+                     cudaStream_t st);
+
+// ---- ESP (ctc_esp.cu) ----
+int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, cudaStream_t st);
+void destroy_esp(ctc_molecule* mol);
+
+// ---- adjoint (ctc_adjoint.cu) ----
+int eval_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const double* v_rho,
+                 const double* v_grad, double* dLdD, double* dLdR, cudaStream_t st);
+
+// chunk size (points) for a given AO footprint
+int64_t chunk_points(const ctc_molecule* mol, int nq_ao);
+
+// status word helpers
+int check_status(ctc_molecule* mol, cudaStream_t st, const char* what);
+
+}  // namespace ctc

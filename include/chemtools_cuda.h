@@ -1,0 +1,171 @@
+/* chemtools_cuda.h -- C ABI of the B200-native grid-evaluation library.
+ *
+ * Drop-in boundary for ChemToolsCUDA's grid-evaluation hot path.  Every entry
+ * point is extern "C", takes plain pointers and sizes, and returns 0 on
+ * success or a negative CTC_ERR_* code; ctc_last_error() then describes the
+ * failure (per calling thread).  Nothing here allocates device memory that
+ * outlives the molecule handle, and no call keeps global device state: each
+ * handle owns its device copy of the basis and density matrix.
+ *
+ * Device-pointer entry points are stream-ordered on the stream passed in
+ * (NULL = legacy default stream) and return before the work finishes.  The
+ * *_host variants take host pointers, copy inputs and outputs themselves and
+ * return after the results are in host memory.
+ *
+ * Layouts: points are row-major (N, 3) doubles; gradients (N, 3); Hessians
+ * (N, 3, 3); scalar descriptors (N,).  AO functions follow the reference's
+ * order: shells in input order, segments in order, and within a segment the
+ * Cartesian order xx,yy,zz,xy,xz,yz (d), xxx,yyy,zzz,xyy,xxy,xxz,xzz,yzz,yyz,xyz
+ * (f), zzzz,yzzz,...,xxxx (g), or the pure order c0,c1,s1,c2,s2,... .
+ */
+#ifndef CHEMTOOLS_CUDA_B200_H_
+#define CHEMTOOLS_CUDA_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes --------------------------------------------------------------------------- */
+#define CTC_OK 0
+#define CTC_ERR_INVALID (-1)     /* bad argument (null pointer, size, angular momentum, ...) */
+#define CTC_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define CTC_ERR_UNSUPPORTED (-3) /* feature not available for this input / device */
+#define CTC_ERR_NOMEM (-4)       /* device or pinned-host allocation failed */
+#define CTC_ERR_DEVICE (-5)      /* a kernel reported an error through its status word */
+
+/* ---- precision of the Phi*D contraction ------------------------------------------------------ */
+#define CTC_PREC_FP64 0      /* FP64 throughout (double-precision matrix units) */
+#define CTC_PREC_TC_SPLIT 1  /* INT8 tensor cores, 4-way split operands, exact int32 accumulation */
+
+typedef struct ctc_molecule ctc_molecule; /* opaque handle */
+
+/* Contracted Gaussian basis in the reference's generalised-contraction form
+ * (include/contracted_shell.h:39-44): shell s has nprim[s] exponents shared by
+ * nseg[s] segments; segment g has angular momentum angmoms[...] in the fchk
+ * code (0 s, 1 p, 2 Cartesian d, -2 pure d, 3/-3 f, 4/-4 g) and coefficients
+ * coeffs[off + g*nprim[s] + k] of L2-normalised primitives.  shell_atom may be
+ * NULL, in which case shells are attached to the atom at their centre. */
+typedef struct {
+  int32_t nshell;
+  const double* centers;     /* [nshell][3] bohr */
+  const int32_t* shell_atom; /* [nshell] or NULL */
+  const int32_t* nprim;      /* [nshell] */
+  const int32_t* nseg;       /* [nshell] */
+  const int32_t* angmoms;    /* [sum nseg] */
+  const double* exps;        /* [sum nprim] */
+  const double* coeffs;      /* [sum nseg*nprim] */
+} ctc_basis;
+
+/* Output slots of the local-descriptor evaluation.  A NULL slot is not
+ * computed; the kernels then skip the derivatives and products that only it
+ * needs. */
+typedef struct {
+  double* rho;          /* (N)     electron density */
+  double* grad;         /* (N,3)   gradient of rho */
+  double* hess;         /* (N,3,3) Hessian of rho */
+  double* lap;          /* (N)     Laplacian of rho */
+  double* tau_pd;       /* (N)     positive-definite kinetic-energy density */
+  double* tau_alpha;    /* (N)     tau_pd + alpha * lap */
+  double* rdg;          /* (N)     reduced density gradient */
+  double* shannon;      /* (N)     rho * ln(rho) */
+  double* weizsacker;   /* (N)     |grad rho|^2 / (8 rho) */
+  double* thomas_fermi; /* (N)     3/10 (3 pi^2)^(2/3) rho^(5/3) */
+  double* gge;          /* (N)     thomas_fermi + gge_a * weizsacker + gge_b * lap */
+  double* general_ked;  /* (N)     tau_pd + (ked_a - 1)/4 * lap */
+} ctc_outputs;
+
+typedef struct {
+  double alpha;        /* tau_alpha parameter */
+  double gge_a, gge_b; /* general gradient-expansion parameters */
+  double ked_a;        /* general(ish) KED parameter */
+} ctc_params;
+
+/* ---- molecule ------------------------------------------------------------------------------ */
+
+/* Build a molecule on the current device: basis tables, density matrix D
+ * (nbasis x nbasis, row-major, symmetric, host memory), atoms (host).
+ * Replaces the IOData/MolecularBasis set-up of the reference
+ * (include/iodata.h:34-38, src/iodata.cpp:15-211) and the constant-memory
+ * upload (src/basis_to_gpu.cu:16-166, include/basis_to_gpu.cuh:42). */
+int ctc_molecule_create(const ctc_basis* basis, int32_t natom, const double* atom_xyz,
+                        const double* atom_charges, const double* D, int32_t nbasis,
+                        ctc_molecule** out);
+int ctc_molecule_destroy(ctc_molecule* mol);
+int ctc_molecule_nbasis(const ctc_molecule* mol);
+int ctc_molecule_natom(const ctc_molecule* mol);
+
+/* Replace D from device memory (stream-ordered).  Replaces the per-call
+ * cublasSetMatrix uploads (e.g. src/evaluate_density.cu:777). */
+int ctc_molecule_set_density_matrix(ctc_molecule* mol, const double* d_D, void* stream);
+
+/* Move the atoms (host (natom,3)); the shells move with their atoms. */
+int ctc_molecule_set_coordinates(ctc_molecule* mol, const double* atom_xyz);
+
+/* Make every table the evaluation needs resident on the device now (the
+ * split-precision copy of D included).  Idempotent.  Replaces
+ * Molecule::basis_set_to_constant_memory (src/pymolecule.cu:25-32). */
+int ctc_molecule_prepare(ctc_molecule* mol, int32_t precision);
+
+/* ---- local descriptors --------------------------------------------------------------------- */
+
+/* All requested local descriptors at N points in one fused pass.  Replaces
+ * evaluate_electron_density_on_any_grid (include/evaluate_density.cuh:113),
+ * evaluate_electron_density_gradient (include/evaluate_gradient.cuh:95),
+ * evaluate_electron_density_hessian (include/evaluate_hessian.cuh:88),
+ * evaluate_laplacian (include/evaluate_laplacian.cuh:97),
+ * evaluate_positive_definite_kinetic_density and
+ * evaluate_general_kinetic_energy_density (include/evaluate_kinetic_dens.cuh:27,45),
+ * and compute_reduced_density_gradient, compute_weizsacker_ked,
+ * compute_thomas_fermi_energy_density, compute_ked_gradient_expansion_general,
+ * compute_general_ked, compute_shannon_information_density
+ * (include/evaluate_densbased.cuh:31-103). */
+int ctc_eval_local(ctc_molecule* mol, const double* d_points, int64_t npoints, int32_t precision,
+                   const ctc_params* params, const ctc_outputs* d_out, void* stream);
+
+/* Same with host points and host outputs; copies are inside the call. */
+int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t npoints,
+                        int32_t precision, const ctc_params* params, const ctc_outputs* h_out);
+
+/* Descriptors on a cubic grid generated on the device: point (i,j,k) =
+ * origin + i*axes[0..2] + j*axes[3..5] + k*axes[6..8], k fastest, outputs in
+ * (shape[0], shape[1], shape[2]) C order.  Replaces
+ * evaluate_electron_density_on_cubic (include/evaluate_density.cuh:100). */
+int ctc_eval_cubic(ctc_molecule* mol, const double* origin, const double* axes,
+                   const int32_t* shape, int32_t precision, const ctc_params* params,
+                   const ctc_outputs* d_out, void* stream);
+
+/* AO values and derivatives, out (nq, N, nbasis) with nq = 1, 4 or 10 for
+ * deriv = 0, 1, 2 (value, x, y, z, xx, xy, xz, yy, yz, zz).  Replaces
+ * evaluate_contraction_derivatives (include/evaluate_gradient.cuh:61) and
+ * evaluate_contraction_second_derivative (include/evaluate_hessian.cuh:56). */
+int ctc_eval_ao(ctc_molecule* mol, const double* d_points, int64_t npoints, int32_t deriv,
+                double* d_out, void* stream);
+
+/* ---- electrostatic potential ------------------------------------------------------------- */
+
+/* V(r) = sum_A Z_A/|r - R_A| - sum_{mu nu} D_{mu nu} (mu|1/|r - r'||nu) at N
+ * points.  Replaces compute_electrostatic_potential_over_points
+ * (include/evaluate_electrostatic.cuh:37).  Shells up to g are supported. */
+int ctc_eval_esp(ctc_molecule* mol, const double* d_points, int64_t npoints, double* d_out,
+                 void* stream);
+int ctc_eval_esp_host(ctc_molecule* mol, const double* h_points, int64_t npoints, double* h_out);
+
+/* ---- adjoint (no counterpart in the reference) --------------------------------------------- */
+
+/* Given v_rho = dL/drho (N) and v_grad = dL/d(grad rho) (N,3, may be NULL)
+ * at N points, accumulate (+=) dL/dD (nbasis x nbasis, entries treated as
+ * independent) and dL/dR (natom x 3, points and weights held fixed).  Either
+ * output may be NULL.  Device pointers, stream-ordered. */
+int ctc_adjoint(ctc_molecule* mol, const double* d_points, int64_t npoints, const double* d_v_rho,
+                const double* d_v_grad, double* d_dLdD, double* d_dLdR, void* stream);
+
+/* ---- misc ---------------------------------------------------------------------------------- */
+const char* ctc_last_error(void);
+const char* ctc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHEMTOOLS_CUDA_B200_H_ */

@@ -1,0 +1,213 @@
+// ref_harness.cu -- TEST INFRASTRUCTURE ONLY.
+//
+// A thin extern "C" shim over the reference's own host drivers so that tests
+// and the benchmark's reference arm can call the reference's CUDA code, built
+// from its unmodified sources by oracle/Makefile (`make -C oracle ref`), on
+// synthetic molecules.  The reference normally builds its IOData through the
+// Python `iodata` package (src/iodata.cpp:15-211); here the public IOData
+// constructor (include/iodata.h:34-38) is fed raw arrays instead, allocated
+// with new[] because the destructor deletes them (include/iodata.h:39-42).
+//
+// Points arrive row-major (N,3) as numpy holds them and are transposed to the
+// column-major layout the drivers expect (e.g. include/evaluate_density.cuh:108),
+// except for the ESP, which takes row-major points (src/pymolecule.cu:129-139).
+//
+// Every entry point catches the reference's exceptions (cudaError_t or
+// std::runtime_error) and returns -1 with a message for ref_last_error().
+#include <cstring>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "contracted_shell.h"
+#include "iodata.h"
+#include "basis_to_gpu.cuh"
+#include "evaluate_density.cuh"
+#include "evaluate_gradient.cuh"
+#include "evaluate_hessian.cuh"
+#include "evaluate_laplacian.cuh"
+#include "evaluate_kinetic_dens.cuh"
+#include "evaluate_densbased.cuh"
+#include "evaluate_electrostatic.cuh"
+
+namespace {
+thread_local std::string g_err;
+
+struct RefMol {
+  chemtools::IOData* io;
+  int M;
+};
+
+std::vector<double> col_major(const double* pts, int n) {
+  std::vector<double> c(3 * (size_t)n);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) c[(size_t)k * n + i] = pts[3 * (size_t)i + k];
+  return c;
+}
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { g_err = cudaGetErrorString(e); return -1; }
+    return 0;
+  } catch (cudaError_t e) {
+    g_err = std::string("cuda error: ") + cudaGetErrorString(e);
+  } catch (std::exception& e) {
+    g_err = e.what();
+  } catch (...) {
+    g_err = "unknown exception";
+  }
+  return -1;
+}
+
+void copy_out(const std::vector<double>& v, double* out) {
+  std::memcpy(out, v.data(), sizeof(double) * v.size());
+}
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err.c_str(); }
+
+// Zero a large block of device memory and release it, so that the drivers'
+// un-zeroed cudaMalloc accumulators (src/evaluate_gradient.cu:1156,1271,1295,
+// src/evaluate_hessian.cu:1863,1922,2091,2115, src/evaluate_kinetic_dens.cu:90)
+// are most likely handed clean pages.  Call once per fresh process.
+int ref_prime_allocator(size_t bytes) {
+  return guard([&] {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) throw std::runtime_error("prime malloc failed");
+    cudaMemset(p, 0, bytes);
+    cudaDeviceSynchronize();
+    cudaFree(p);
+  });
+}
+
+void* ref_create(int nshell, const double* centers, const int* nprim, const int* nseg,
+                 const int* angmoms, const double* exps, const double* coeffs, int natom,
+                 const double* atom_xyz, const double* charges, const double* D, int M) {
+  std::vector<chemtools::GeneralizedContractionShell> shells;
+  int ia = 0, ip = 0, ic = 0;
+  for (int s = 0; s < nshell; ++s) {
+    chemtools::GeneralizedContractionShell sh;
+    int K = nprim[s], S = nseg[s];
+    for (int g = 0; g < S; ++g) sh.angmoms.push_back(angmoms[ia + g]);
+    sh.coordinate = {centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]};
+    for (int k = 0; k < K; ++k) sh.exponents.push_back(exps[ip + k]);
+    for (int g = 0; g < S; ++g) {
+      std::vector<double> c;
+      for (int k = 0; k < K; ++k) c.push_back(coeffs[ic + g * K + k]);
+      sh.coefficients.push_back(c);
+    }
+    shells.push_back(sh);
+    ia += S; ip += K; ic += S * K;
+  }
+  chemtools::MolecularBasis basis(shells);
+  if (basis.numb_basis_functions() != M) { g_err = "basis size does not match D"; return nullptr; }
+  double* coord = new double[3 * natom];
+  std::memcpy(coord, atom_xyz, sizeof(double) * 3 * natom);
+  int* chg = new int[natom];
+  int* num = new int[natom];
+  for (int a = 0; a < natom; ++a) { chg[a] = (int)charges[a]; num[a] = (int)charges[a]; }
+  double* rdm = new double[(size_t)M * M];
+  double* mo_rdm = new double[(size_t)M * M];
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < M; ++j) {
+      rdm[i + (size_t)j * M] = D[(size_t)i * M + j];     // column-major copy
+      mo_rdm[i + (size_t)j * M] = D[(size_t)i * M + j];
+    }
+  double* mo = new double[(size_t)M * M]();
+  double* occ = new double[M]();
+  RefMol* r = new RefMol{new chemtools::IOData(basis, coord, natom, rdm, {M, M}, mo, occ, chg, num,
+                                               mo_rdm), M};
+  return r;
+}
+
+void ref_destroy(void* h) {
+  RefMol* r = (RefMol*)h;
+  delete r->io;
+  delete r;
+}
+
+#define REF_LOCAL(name, call)                                                    \
+  int name(void* h, const double* pts, int n, double* out) {                    \
+    RefMol* r = (RefMol*)h;                                                      \
+    return guard([&] {                                                           \
+      std::vector<double> c = col_major(pts, n);                                 \
+      copy_out(call, out);                                                       \
+    });                                                                          \
+  }
+
+REF_LOCAL(ref_density, chemtools::evaluate_electron_density_on_any_grid(*r->io, c.data(), n))
+REF_LOCAL(ref_gradient, chemtools::evaluate_electron_density_gradient(*r->io, c.data(), n, true))
+REF_LOCAL(ref_hessian, chemtools::evaluate_electron_density_hessian(*r->io, c.data(), n, true))
+REF_LOCAL(ref_laplacian, chemtools::evaluate_laplacian(*r->io, c.data(), n))
+REF_LOCAL(ref_tau_pd, chemtools::evaluate_positive_definite_kinetic_density(*r->io, c.data(), n))
+REF_LOCAL(ref_rdg, chemtools::compute_reduced_density_gradient(*r->io, c.data(), n))
+REF_LOCAL(ref_shannon, chemtools::compute_shannon_information_density(*r->io, c.data(), n))
+REF_LOCAL(ref_weizsacker, chemtools::compute_weizsacker_ked(*r->io, c.data(), n))
+REF_LOCAL(ref_thomas_fermi, chemtools::compute_thomas_fermi_energy_density(*r->io, c.data(), n))
+REF_LOCAL(ref_ao_deriv, chemtools::evaluate_contraction_derivatives(*r->io, c.data(), n))
+REF_LOCAL(ref_ao_sec_deriv, chemtools::evaluate_contraction_second_derivative(*r->io, c.data(), n))
+REF_LOCAL(ref_ao_laplacian,
+          chemtools::evaluate_sum_of_second_derivative_contractions(*r->io, c.data(), n))
+
+// tau_alpha = tau_PD + alpha * lap (src/evaluate_kinetic_dens.cu:195-214)
+int ref_tau_general(void* h, const double* pts, int n, double alpha, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    std::vector<double> c = col_major(pts, n);
+    copy_out(chemtools::evaluate_general_kinetic_energy_density(*r->io, alpha, c.data(), n), out);
+  });
+}
+
+// tau_PD + (a - 1)/4 lap (src/evaluate_densbased.cu:195-208)
+int ref_general_ked(void* h, const double* pts, int n, double a, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    std::vector<double> c = col_major(pts, n);
+    copy_out(chemtools::compute_general_ked(*r->io, c.data(), n, a), out);
+  });
+}
+
+// TF + a W + b lap (src/evaluate_densbased.cu:175-193)
+int ref_gge(void* h, const double* pts, int n, double a, double b, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    std::vector<double> c = col_major(pts, n);
+    copy_out(chemtools::compute_ked_gradient_expansion_general(*r->io, c.data(), n, a, b), out);
+  });
+}
+
+// ESP takes row-major points (src/pymolecule.cu:129-139).
+int ref_esp(void* h, const double* pts, int n, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    std::vector<double> p(pts, pts + 3 * (size_t)n);
+    copy_out(chemtools::compute_electrostatic_potential_over_points(*r->io, p.data(), n, 1e-11,
+                                                                    false), out);
+  });
+}
+
+// Cubic grid: axes row-major (row i = axis i), shape (nx, ny, nz), z fastest.
+// The driver relies on a prior basis upload (src/evaluate_density.cu:462-464),
+// done here as Molecule::basis_set_to_constant_memory does (src/pymolecule.cu:25-32).
+int ref_cubic(void* h, const double* origin, const double* axes, const int* shape, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    chemtools::add_mol_basis_to_constant_memory_array(r->io->GetOrbitalBasis(), false, false);
+    double col[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) col[i + 3 * j] = axes[3 * i + j];
+    copy_out(chemtools::evaluate_electron_density_on_cubic(
+                 *r->io, {origin[0], origin[1], origin[2]}, col, {shape[0], shape[1], shape[2]}, false),
+             out);
+  });
+}
+
+}  // extern "C"

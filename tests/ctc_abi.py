@@ -1,0 +1,204 @@
+"""ctypes view of include/chemtools_cuda.h for the tests.
+
+The GPU parity tests call the library through this C ABI (not through the
+pybind11 module) with torch CUDA tensors as device memory.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "chemtools_cuda.h")
+LIB = os.path.join(ROOT, "chemtoolscuda_b200", "libchemtools_cuda.so")
+
+OUT_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon", "weizsacker",
+            "thomas_fermi", "gge", "general_ked")
+OUT_WIDTH = dict(rho=1, grad=3, hess=9, lap=1, tau_pd=1, tau_alpha=1, rdg=1, shannon=1,
+                 weizsacker=1, thomas_fermi=1, gge=1, general_ked=1)
+PREC_FP64, PREC_TC = 0, 1
+
+
+class Basis(C.Structure):
+    _fields_ = [("nshell", C.c_int32), ("centers", C.c_void_p), ("shell_atom", C.c_void_p),
+                ("nprim", C.c_void_p), ("nseg", C.c_void_p), ("angmoms", C.c_void_p),
+                ("exps", C.c_void_p), ("coeffs", C.c_void_p)]
+
+
+class Outputs(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in OUT_KEYS]
+
+
+class Params(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("gge_a", C.c_double), ("gge_b", C.c_double),
+                ("ked_a", C.c_double)]
+
+
+def header_symbols() -> list[str]:
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(ctc_[a-z0-9_]+)\s*\(", txt)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(LIB)
+        vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+        L = _lib
+        L.ctc_last_error.restype = C.c_char_p
+        L.ctc_version.restype = C.c_char_p
+        L.ctc_molecule_create.argtypes = [vp, i32, vp, vp, vp, i32, vp]
+        L.ctc_molecule_destroy.argtypes = [vp]
+        L.ctc_molecule_nbasis.argtypes = [vp]
+        L.ctc_molecule_natom.argtypes = [vp]
+        L.ctc_molecule_set_density_matrix.argtypes = [vp, vp, vp]
+        L.ctc_molecule_set_coordinates.argtypes = [vp, vp]
+        L.ctc_molecule_prepare.argtypes = [vp, i32]
+        L.ctc_eval_local.argtypes = [vp, vp, i64, i32, vp, vp, vp]
+        L.ctc_eval_local_host.argtypes = [vp, vp, i64, i32, vp, vp]
+        L.ctc_eval_cubic.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp]
+        L.ctc_eval_ao.argtypes = [vp, vp, i64, i32, vp, vp]
+        L.ctc_eval_esp.argtypes = [vp, vp, i64, vp, vp]
+        L.ctc_eval_esp_host.argtypes = [vp, vp, i64, vp]
+        L.ctc_adjoint.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp]
+    return _lib
+
+
+def err() -> str:
+    return lib().ctc_last_error().decode()
+
+
+def check(rc: int, what: str = "call"):
+    if rc != 0:
+        raise RuntimeError(f"{what} -> {rc}: {err()}")
+
+
+class Mol:
+    """Owns a ctc_molecule built from a flat basis (synthetic.flatten_basis layout)."""
+
+    def __init__(self, flat: dict, coords, charges, D, shell_atom: bool = True):
+        self.keep = dict(
+            centers=np.ascontiguousarray(flat["centers"], np.float64),
+            shell_atom=np.ascontiguousarray(flat["shell_atom"], np.int32),
+            nprim=np.ascontiguousarray(flat["nprim"], np.int32),
+            nseg=np.ascontiguousarray(flat["nseg"], np.int32),
+            angmoms=np.ascontiguousarray(flat["angmoms"], np.int32),
+            exps=np.ascontiguousarray(flat["exps"], np.float64),
+            coeffs=np.ascontiguousarray(flat["coeffs"], np.float64),
+            coords=np.ascontiguousarray(coords, np.float64),
+            charges=np.ascontiguousarray(charges, np.float64),
+            D=np.ascontiguousarray(D, np.float64))
+        k = self.keep
+        b = Basis(len(k["nprim"]), k["centers"].ctypes.data,
+                  k["shell_atom"].ctypes.data if shell_atom else None, k["nprim"].ctypes.data,
+                  k["nseg"].ctypes.data, k["angmoms"].ctypes.data, k["exps"].ctypes.data,
+                  k["coeffs"].ctypes.data)
+        h = C.c_void_p()
+        check(lib().ctc_molecule_create(C.byref(b), len(k["coords"]), k["coords"].ctypes.data,
+                                        k["charges"].ctypes.data, k["D"].ctypes.data,
+                                        k["D"].shape[0], C.byref(h)), "ctc_molecule_create")
+        self.h = h
+        self.M = k["D"].shape[0]
+
+    def close(self):
+        if self.h:
+            lib().ctc_molecule_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- device helpers (torch) ----
+    def eval_local(self, points, keys, precision=PREC_FP64, params=(0.5, 1 / 9, 1 / 6, 1.0)):
+        import torch
+        pts = torch.as_tensor(np.ascontiguousarray(points), dtype=torch.float64, device="cuda")
+        n = pts.shape[0]
+        outs = {k: torch.full((n * OUT_WIDTH[k],), float("nan"), dtype=torch.float64, device="cuda")
+                for k in keys}
+        o = Outputs(**{k: outs[k].data_ptr() for k in keys})
+        p = Params(*params)
+        check(lib().ctc_eval_local(self.h, pts.data_ptr(), n, precision, C.byref(p), C.byref(o),
+                                   None), "ctc_eval_local")
+        torch.cuda.synchronize()
+        res = {}
+        for k, t in outs.items():
+            a = t.cpu().numpy()
+            res[k] = a.reshape(n, 3) if k == "grad" else (a.reshape(n, 3, 3) if k == "hess" else a)
+        return res
+
+    def eval_local_host(self, points, keys, precision=PREC_FP64, params=(0.5, 1 / 9, 1 / 6, 1.0)):
+        pts = np.ascontiguousarray(points, np.float64)
+        n = len(pts)
+        outs = {k: np.full(n * OUT_WIDTH[k], np.nan) for k in keys}
+        o = Outputs(**{k: outs[k].ctypes.data for k in keys})
+        p = Params(*params)
+        check(lib().ctc_eval_local_host(self.h, pts.ctypes.data, n, precision, C.byref(p),
+                                        C.byref(o)), "ctc_eval_local_host")
+        return {k: (a.reshape(n, 3) if k == "grad" else (a.reshape(n, 3, 3) if k == "hess" else a))
+                for k, a in outs.items()}
+
+    def eval_cubic(self, origin, axes, shape, keys=("rho",), precision=PREC_FP64):
+        import torch
+        n = int(np.prod(shape))
+        outs = {k: torch.full((n * OUT_WIDTH[k],), float("nan"), dtype=torch.float64, device="cuda")
+                for k in keys}
+        o = Outputs(**{k: outs[k].data_ptr() for k in keys})
+        org = np.ascontiguousarray(origin, np.float64)
+        ax = np.ascontiguousarray(axes, np.float64)
+        sh = np.ascontiguousarray(shape, np.int32)
+        check(lib().ctc_eval_cubic(self.h, org.ctypes.data, ax.ctypes.data, sh.ctypes.data,
+                                   precision, None, C.byref(o), None), "ctc_eval_cubic")
+        torch.cuda.synchronize()
+        return {k: t.cpu().numpy() for k, t in outs.items()}
+
+    def eval_ao(self, points, deriv):
+        import torch
+        pts = torch.as_tensor(np.ascontiguousarray(points), dtype=torch.float64, device="cuda")
+        n = pts.shape[0]
+        nq = {0: 1, 1: 4, 2: 10}[deriv]
+        out = torch.full((nq, n, self.M), float("nan"), dtype=torch.float64, device="cuda")
+        check(lib().ctc_eval_ao(self.h, pts.data_ptr(), n, deriv, out.data_ptr(), None), "ctc_eval_ao")
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    def eval_esp(self, points):
+        import torch
+        pts = torch.as_tensor(np.ascontiguousarray(points), dtype=torch.float64, device="cuda")
+        out = torch.full((pts.shape[0],), float("nan"), dtype=torch.float64, device="cuda")
+        check(lib().ctc_eval_esp(self.h, pts.data_ptr(), pts.shape[0], out.data_ptr(), None),
+              "ctc_eval_esp")
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    def eval_esp_host(self, points):
+        pts = np.ascontiguousarray(points, np.float64)
+        out = np.full(len(pts), np.nan)
+        check(lib().ctc_eval_esp_host(self.h, pts.ctypes.data, len(pts), out.ctypes.data),
+              "ctc_eval_esp_host")
+        return out
+
+    def adjoint(self, points, v_rho, v_grad=None, want_D=True, want_R=True):
+        import torch
+        dev = "cuda"
+        pts = torch.as_tensor(np.ascontiguousarray(points), dtype=torch.float64, device=dev)
+        vr = torch.as_tensor(np.ascontiguousarray(v_rho), dtype=torch.float64, device=dev)
+        vg = None if v_grad is None else torch.as_tensor(np.ascontiguousarray(v_grad),
+                                                          dtype=torch.float64, device=dev)
+        natom = len(self.keep["coords"])
+        dD = torch.zeros((self.M, self.M), dtype=torch.float64, device=dev) if want_D else None
+        dR = torch.zeros((natom, 3), dtype=torch.float64, device=dev) if want_R else None
+        check(lib().ctc_adjoint(self.h, pts.data_ptr(), pts.shape[0], vr.data_ptr(),
+                                None if vg is None else vg.data_ptr(),
+                                None if dD is None else dD.data_ptr(),
+                                None if dR is None else dR.data_ptr(), None), "ctc_adjoint")
+        torch.cuda.synchronize()
+        return (None if dD is None else dD.cpu().numpy(), None if dR is None else dR.cpu().numpy())
