@@ -91,7 +91,7 @@ def eval_ao(flat: dict, points: np.ndarray, deriv: int = 0, nthreads: int = 0) -
     return out
 
 
-LOCAL_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_a", "rdg", "shannon")
+LOCAL_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon")
 
 
 def eval_local(flat: dict, D: np.ndarray, points: np.ndarray, alpha: float = 0.5,
@@ -100,7 +100,7 @@ def eval_local(flat: dict, D: np.ndarray, points: np.ndarray, alpha: float = 0.5
     pts = np.ascontiguousarray(points, np.float64)
     Dm = np.ascontiguousarray(D, np.float64)
     n = len(pts)
-    shapes = dict(rho=(n,), grad=(n, 3), hess=(n, 3, 3), lap=(n,), tau_pd=(n,), tau_a=(n,),
+    shapes = dict(rho=(n,), grad=(n, 3), hess=(n, 3, 3), lap=(n,), tau_pd=(n,), tau_alpha=(n,),
                   rdg=(n,), shannon=(n,))
     out = {k: np.zeros(shapes[k]) for k in keys}
     rc = lib().ctco_eval_local(b.ptr, _p(Dm), Dm.shape[0], _p(pts), n, float(alpha),

@@ -48,11 +48,15 @@ std::vector<double> col_major(const double* pts, int n) {
   return c;
 }
 
+// tolerate_invalid_value: the Hessian driver frees d_contractions twice
+// (src/evaluate_hessian.cu:2173 and :2230) after its results are complete,
+// which leaves cudaErrorInvalidValue as the last error.
 template <class F>
-int guard(F&& f) {
+int guard(F&& f, bool tolerate_invalid_value = false) {
   try {
     f();
     cudaError_t e = cudaGetLastError();
+    if (e == cudaErrorInvalidValue && tolerate_invalid_value) return 0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); return -1; }
     return 0;
   } catch (cudaError_t e) {
@@ -145,7 +149,6 @@ void ref_destroy(void* h) {
 
 REF_LOCAL(ref_density, chemtools::evaluate_electron_density_on_any_grid(*r->io, c.data(), n))
 REF_LOCAL(ref_gradient, chemtools::evaluate_electron_density_gradient(*r->io, c.data(), n, true))
-REF_LOCAL(ref_hessian, chemtools::evaluate_electron_density_hessian(*r->io, c.data(), n, true))
 REF_LOCAL(ref_laplacian, chemtools::evaluate_laplacian(*r->io, c.data(), n))
 REF_LOCAL(ref_tau_pd, chemtools::evaluate_positive_definite_kinetic_density(*r->io, c.data(), n))
 REF_LOCAL(ref_rdg, chemtools::compute_reduced_density_gradient(*r->io, c.data(), n))
@@ -156,6 +159,14 @@ REF_LOCAL(ref_ao_deriv, chemtools::evaluate_contraction_derivatives(*r->io, c.da
 REF_LOCAL(ref_ao_sec_deriv, chemtools::evaluate_contraction_second_derivative(*r->io, c.data(), n))
 REF_LOCAL(ref_ao_laplacian,
           chemtools::evaluate_sum_of_second_derivative_contractions(*r->io, c.data(), n))
+
+int ref_hessian(void* h, const double* pts, int n, double* out) {
+  RefMol* r = (RefMol*)h;
+  return guard([&] {
+    std::vector<double> c = col_major(pts, n);
+    copy_out(chemtools::evaluate_electron_density_hessian(*r->io, c.data(), n, true), out);
+  }, true);
+}
 
 // tau_alpha = tau_PD + alpha * lap (src/evaluate_kinetic_dens.cu:195-214)
 int ref_tau_general(void* h, const double* pts, int n, double alpha, double* out) {

@@ -76,7 +76,22 @@ def case_esp():
     return mol, pts
 
 
-CASES = {"allshell": case_allshell, "c1": case_c1, "esp": case_esp}
+def case_mixed():
+    """Pure g, Cartesian and pure f, Cartesian and pure d, generalised s+p and
+    d+5d shells -- every type whose first derivatives the reference gets right
+    (its Cartesian-g first derivatives are defective), so every descriptor is
+    pinned."""
+    rng = np.random.default_rng(14)
+    coords = np.array([[0.0, 0.0, 0.0], [1.7, -0.5, 0.9], [-1.1, 1.2, -0.4], [0.6, 1.9, 1.3]])
+    specs = [(0, [0], 4), (0, [0, 1], 3), (0, [2], 2), (0, [-3], 2), (0, [-4], 2), (1, [0], 3),
+             (1, [1], 2), (1, [2, -2], 2), (1, [3], 2), (1, [-4], 1), (2, [0], 3), (2, [1], 2),
+             (2, [-2], 1), (3, [0], 2), (3, [1], 1)]
+    mol = _molecule(rng, coords, [8, 6, 7, 1], specs, 14, "mixed")
+    pts = _points_away(rng, mol, 192, rmin=0.05)
+    return mol, pts
+
+
+CASES = {"allshell": case_allshell, "c1": case_c1, "esp": case_esp, "mixed": case_mixed}
 # Reference calls made for every case; ESP only where the basis has no g shell.
 LOCAL_FUNCS = ["density", "gradient", "hessian", "laplacian", "tau_pd", "tau_general", "rdg",
                "shannon", "weizsacker", "thomas_fermi", "gge", "general_ked", "ao_deriv",

@@ -40,7 +40,7 @@ def _mol(mol):
     return ctc_abi.Mol(mol.flat(), mol.coords, mol.charges, mol.D)
 
 
-@pytest.mark.parametrize("case", ["allshell", "c1", "esp"])
+@pytest.mark.parametrize("case", ["allshell", "c1", "esp", "mixed"])
 @pytest.mark.parametrize("deriv", [0, 1, 2])
 def test_ao_values_and_derivatives(torch_cuda, case, deriv):
     mol, pts = _cases().CASES[case]()
@@ -52,7 +52,7 @@ def test_ao_values_and_derivatives(torch_cuda, case, deriv):
         assert_close(f"{case} AO q={q}", got[q], ref[q], scale, 1e-12)
 
 
-@pytest.mark.parametrize("case", ["allshell", "c1", "esp"])
+@pytest.mark.parametrize("case", ["allshell", "c1", "esp", "mixed"])
 def test_local_descriptors_fp64_vs_oracle(torch_cuda, case):
     mol, pts = _cases().CASES[case]()
     m = _mol(mol)
@@ -182,7 +182,7 @@ def _golden_mol(g):
     return flat, ctc_abi.Mol(flat, g["in_coords"], g["in_charges"], g["in_D"])
 
 
-@pytest.mark.parametrize("case", ["allshell", "c1", "esp"])
+@pytest.mark.parametrize("case", ["c1", "esp", "mixed"])
 def test_fp64_path_vs_reference_outputs(torch_cuda, case):
     """Directly against what the reference's CUDA drivers returned."""
     g = _golden(case)

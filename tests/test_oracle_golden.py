@@ -1,0 +1,139 @@
+"""Pin the FP64 oracle to the reference: the oracle reproduces the outputs of
+the reference's own CUDA drivers (tests/golden/*.npz, written by
+tests/golden/make_golden.py on a GPU from the reference sources).
+
+Tolerances follow the reference's tests: AO derivatives, gradient and Hessian
+1e-10, density, Laplacian, tau and ESP 1e-8 (tests/test_gradient.cu,
+tests/test_hessian.cu, tests/test_laplacian.cu, tests/test_kinetic_density.cu,
+tests/test_electrostatic_potential.cu), here applied relative to the per-point
+sum of absolute terms (tests/helpers.py) and, for the reference's known
+defects, documented where they show up."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import assert_close, term_scales
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = ["allshell", "c1", "esp", "mixed"]
+
+
+def load(case):
+    p = os.path.join(GOLDEN, f"{case}.npz")
+    if not os.path.exists(p):
+        pytest.skip(f"{case}.npz missing")
+    g = dict(np.load(p))
+    flat = {k[3:]: g[k] for k in ("in_centers", "in_shell_atom", "in_nprim", "in_nseg",
+                                   "in_angmoms", "in_exps", "in_coeffs")}
+    return g, flat
+
+
+def _ao_angmom(flat):
+    from chemtoolscuda_b200.synthetic import nfunc
+    return np.array([a for a in flat["angmoms"] for _ in range(nfunc(int(a)))])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_ao_derivatives_match_reference(case):
+    g, flat = load(case)
+    pts = g["in_points"]
+    ao = O.eval_ao(flat, pts, 2)
+    # reference layouts: (3, M, N), (6, M, N), (M, N)
+    d1 = g["ref_ao_deriv"]
+    keep = _ao_angmom(flat) != 4   # see test_reference_cartesian_g_gradient_defect
+    assert_close("d1", ao[1:4].transpose(0, 2, 1)[:, keep], d1[:, keep], np.abs(d1).max(), 1e-12)
+    d2 = g["ref_ao_sec_deriv"]
+    assert_close("d2", ao[4:10].transpose(0, 2, 1), d2, np.abs(d2).max(), 1e-12)
+    lap = g["ref_ao_laplacian"]
+    mine = (ao[4] + ao[7] + ao[9]).T
+    assert_close("lap", mine, lap, np.abs(lap).max(), 1e-12)
+
+
+def test_reference_cartesian_g_gradient_defect():
+    """Reference defect, documented: the first-derivative code for Cartesian g
+    shells (src/evaluate_gradient.cu:604 onwards) normalises with
+    normalization_primitive_f and writes the components in a permuted order, so
+    its d/dx of a Cartesian g AO is not the derivative of its own AO value.  The
+    reference's second derivatives and Laplacian of the same AOs agree with the
+    oracle to 1e-15 (test above); the oracle keeps the analytic derivative."""
+    g, flat = load("allshell")
+    ao = O.eval_ao(flat, g["in_points"], 1)
+    cart_g = _ao_angmom(flat) == 4
+    d1 = g["ref_ao_deriv"][:, cart_g]
+    mine = ao[1:4].transpose(0, 2, 1)[:, cart_g]
+    assert np.abs(mine - d1).max() > 1e-2 * np.abs(d1).max()
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c != "allshell"])
+def test_local_descriptors_match_reference(case):
+    g, flat = load(case)
+    pts, D = g["in_points"], g["in_D"]
+    a = float(g["meta_tau_alpha"])
+    ref = O.eval_local(flat, D, pts, alpha=a)
+    sc = term_scales(flat, D, pts, alpha=a, ref=ref)
+    assert_close("rho", ref["rho"], g["ref_density"], sc["rho"], 1e-10, 1e-14)
+    assert_close("grad", ref["grad"], g["ref_gradient"], sc["grad"], 1e-10, 1e-14)
+    if "ref_hessian" in g:
+        assert_close("hess", ref["hess"], g["ref_hessian"], sc["hess"], 1e-10, 1e-14)
+    assert_close("lap", ref["lap"], g["ref_laplacian"], sc["lap"], 1e-10, 1e-14)
+    assert_close("tau_pd", ref["tau_pd"], g["ref_tau_pd"], sc["tau_pd"], 1e-10, 1e-14)
+    assert_close("tau_alpha", ref["tau_alpha"], g["ref_tau_general"], sc["tau_alpha"], 1e-10, 1e-14)
+    live = ref["rho"] > 1e-10
+    assert_close("rdg", ref["rdg"], g["ref_rdg"], sc["rdg"], 1e-9, 1e-14, mask=live)
+    assert_close("shannon", ref["shannon"], g["ref_shannon"], sc["shannon"], 1e-10, 1e-14, mask=live)
+
+
+def test_density_with_cartesian_g_matches_reference():
+    """rho uses AO values only, so it is pinned even where the reference's
+    Cartesian-g derivatives are wrong."""
+    g, flat = load("allshell")
+    pts, D = g["in_points"], g["in_D"]
+    ref = O.eval_local(flat, D, pts, keys=("rho", "hess"))
+    sc = term_scales(flat, D, pts)
+    assert_close("rho", ref["rho"], g["ref_density"], sc["rho"], 1e-10, 1e-14)
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c != "allshell"])
+def test_pointwise_kinetic_energy_densities_match_reference(case):
+    g, flat = load(case)
+    pts, D = g["in_points"], g["in_D"]
+    ref = O.eval_local(flat, D, pts, keys=("rho", "grad", "lap", "tau_pd"))
+    rho, lap, tau = ref["rho"], ref["lap"], ref["tau_pd"]
+    g2 = (ref["grad"] ** 2).sum(1)
+    live = rho > 1e-10
+    w = np.where(8 * rho > 1e-20, g2 / (8 * rho), 1e-20)
+    tf = 0.3 * (3 * np.pi ** 2) ** (2 / 3) * rho ** (5 / 3)
+    a, b = g["meta_gge_ab"]
+    ka = float(g["meta_general_ked_a"])
+    np.testing.assert_allclose(w[live], g["ref_weizsacker"][live], rtol=1e-8)
+    np.testing.assert_allclose(tf[live], g["ref_thomas_fermi"][live], rtol=1e-9)
+    sc = term_scales(flat, D, pts, ref=dict(ref, rdg=np.ones_like(rho)))
+    assert_close("gge", tf + a * w + b * lap, g["ref_gge"], sc["gge"], 1e-8, 1e-14, mask=live)
+    assert_close("general_ked", tau + (ka - 1) / 4 * lap, g["ref_general_ked"],
+                 sc["tau_pd"] + abs(ka - 1) / 4 * sc["lap"], 1e-10, 1e-14)
+
+
+@pytest.mark.parametrize("case", ["c1", "esp"])
+def test_esp_matches_reference(case):
+    g, flat = load(case)
+    if "ref_esp" not in g:
+        pytest.skip("no reference ESP for this case")
+    pts = g["in_points"]
+    mine = O.eval_esp(flat, g["in_D"], g["in_coords"], g["in_charges"], pts)
+    nuc = np.array([(g["in_charges"] / np.linalg.norm(g["in_coords"] - p, axis=1)).sum() for p in pts])
+    scale = np.abs(nuc) + np.abs(nuc - g["ref_esp"])
+    assert_close("esp", mine, g["ref_esp"], scale, 1e-8)
+
+
+@pytest.mark.parametrize("case", ["c1", "allshell"])
+def test_cubic_grid_matches_reference(case):
+    g, flat = load(case)
+    if "ref_cubic" not in g:
+        pytest.skip("no reference cubic grid")
+    from chemtoolscuda_b200 import synthetic as S
+    pts = S.cube_points(g["in_cube_origin"], g["in_cube_axes"], tuple(g["in_cube_shape"]))
+    ref = O.eval_local(flat, g["in_D"], pts, keys=("rho",))
+    sc = term_scales(flat, g["in_D"], pts)
+    assert_close("cubic", ref["rho"], g["ref_cubic"].ravel(), sc["rho"], 1e-10, 1e-14)
