@@ -27,92 +27,133 @@ namespace {
 
 constexpr int kAoThreads = 128;
 
+__device__ __forceinline__ int ncomp_dev(int type) {
+  switch (type) {
+    case 0: return 1;
+    case 1: return 3;
+    case 2: return 6;
+    case 3: return 5;
+    case 4: return 10;
+    case 5: return 7;
+    case 6: return 15;
+    default: return 9;
+  }
+}
+
+// Evaluate one segment at one point: o[i * ld_q + j] for quantity i < nq_out
+// and component j.  Outside the screening radius every entry is zero.
+template <int DERIV>
+__device__ __forceinline__ void eval_segment(const DevSeg& sg, const double* __restrict__ alpha,
+                                             const double* __restrict__ coef, double px, double py,
+                                             double pz, double* __restrict__ o, int64_t ld_q,
+                                             int nq_out) {
+  constexpr int NQ = DERIV == 0 ? 1 : (DERIV == 1 ? 4 : 10);
+  const int nc = ncomp_dev(sg.type);
+  const double x = px - sg.cx, y = py - sg.cy, z = pz - sg.cz;
+  const double r2 = x * x + y * y + z * z;
+  if (r2 > sg.rcut2) {
+    for (int q = 0; q < nq_out; ++q)
+      for (int j = 0; j < nc; ++j) o[q * ld_q + j] = 0.0;
+    return;
+  }
+  double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+  for (int k = 0; k < sg.nprim; ++k) {
+    const double a = alpha[sg.prim0 + k];
+    const double e = coef[sg.prim0 + k] * exp(-a * r2);
+    R0 += e;
+    if (DERIV >= 1) R1 += a * e;
+    if (DERIV >= 2) R2 += a * a * e;
+  }
+  // powers with two leading zeros: P[i] = x^(i-2), P[0] = P[1] = 0
+  double X[9], Y[9], Z[9];
+  X[0] = X[1] = Y[0] = Y[1] = Z[0] = Z[1] = 0.0;
+  X[2] = Y[2] = Z[2] = 1.0;
+#pragma unroll
+  for (int i = 3; i < 9; ++i) {
+    X[i] = X[i - 1] * x;
+    Y[i] = Y[i - 1] * y;
+    Z[i] = Z[i - 1] * z;
+  }
+  for (int j = 0; j < nc; ++j) {
+    double q[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) q[i] = 0.0;
+    const int tb = c_comp_off[sg.type][j], te = c_comp_off[sg.type][j + 1];
+    for (int t = tb; t < te; ++t) {
+      const Term T = c_terms[t];
+      const int a = T.a, b = T.b, c = T.z;
+      const double X0 = X[a + 2], Y0 = Y[b + 2], Z0 = Z[c + 2];
+      q[0] += T.c * X0 * Y0 * Z0 * R0;
+      if (DERIV >= 1) {
+        const double Xa = a * X[a + 1], Xb = X[a + 3];
+        const double Ya = b * Y[b + 1], Yb = Y[b + 3];
+        const double Za = c * Z[c + 1], Zb = Z[c + 3];
+        q[1] += T.c * Y0 * Z0 * (Xa * R0 - 2.0 * Xb * R1);
+        q[2] += T.c * X0 * Z0 * (Ya * R0 - 2.0 * Yb * R1);
+        q[3] += T.c * X0 * Y0 * (Za * R0 - 2.0 * Zb * R1);
+        if (DERIV >= 2) {
+          const double Xaa = a * (a - 1) * X[a], Xd = X[a + 4];
+          const double Yaa = b * (b - 1) * Y[b], Yd = Y[b + 4];
+          const double Zaa = c * (c - 1) * Z[c], Zd = Z[c + 4];
+          q[4] += T.c * Y0 * Z0 * (Xaa * R0 - 2.0 * (2 * a + 1) * X0 * R1 + 4.0 * Xd * R2);
+          q[5] += T.c * Z0 * (Xa * Ya * R0 - 2.0 * (Xa * Yb + Xb * Ya) * R1 + 4.0 * Xb * Yb * R2);
+          q[6] += T.c * Y0 * (Xa * Za * R0 - 2.0 * (Xa * Zb + Xb * Za) * R1 + 4.0 * Xb * Zb * R2);
+          q[7] += T.c * X0 * Z0 * (Yaa * R0 - 2.0 * (2 * b + 1) * Y0 * R1 + 4.0 * Yd * R2);
+          q[8] += T.c * X0 * (Ya * Za * R0 - 2.0 * (Ya * Zb + Yb * Za) * R1 + 4.0 * Yb * Zb * R2);
+          q[9] += T.c * X0 * Y0 * (Zaa * R0 - 2.0 * (2 * c + 1) * Z0 * R1 + 4.0 * Zd * R2);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NQ; ++i)
+      if (i < nq_out) o[i * ld_q + j] = q[i];
+  }
+}
+
 template <int DERIV>
 __global__ void __launch_bounds__(kAoThreads)
     ao_kernel(const DevSeg* __restrict__ segs, const int32_t* __restrict__ order, int nseg,
               const double* __restrict__ alpha, const double* __restrict__ coef, PointSrc src,
               int64_t n, int ppb, double* __restrict__ out, int nq_out, int64_t ld_point,
               int64_t ld_q) {
-  constexpr int NQ = DERIV == 0 ? 1 : (DERIV == 1 ? 4 : 10);
   int si = blockIdx.x * kAoThreads + threadIdx.x;
   if (si >= nseg) return;
   const DevSeg sg = segs[order[si]];
-  int nc;
-  switch (sg.type) {
-    case 0: nc = 1; break;
-    case 1: nc = 3; break;
-    case 2: nc = 6; break;
-    case 3: nc = 5; break;
-    case 4: nc = 10; break;
-    case 5: nc = 7; break;
-    case 6: nc = 15; break;
-    default: nc = 9; break;
-  }
   int64_t p_begin = (int64_t)blockIdx.y * ppb;
   int64_t p_end = min(p_begin + ppb, n);
   for (int64_t p = p_begin; p < p_end; ++p) {
     double px, py, pz;
     point_of(src, p, px, py, pz);
-    double x = px - sg.cx, y = py - sg.cy, z = pz - sg.cz;
-    double r2 = x * x + y * y + z * z;
-    double* o = out + p * ld_point + sg.ao0;
-    if (r2 > sg.rcut2) {
-      for (int q = 0; q < nq_out; ++q)
-        for (int j = 0; j < nc; ++j) o[q * ld_q + j] = 0.0;
-      continue;
-    }
-    double R0 = 0.0, R1 = 0.0, R2 = 0.0;
-    for (int k = 0; k < sg.nprim; ++k) {
-      double a = alpha[sg.prim0 + k];
-      double e = coef[sg.prim0 + k] * exp(-a * r2);
-      R0 += e;
-      if (DERIV >= 1) R1 += a * e;
-      if (DERIV >= 2) R2 += a * a * e;
-    }
-    // powers with two leading zeros: P[i] = x^(i-2), P[0] = P[1] = 0
-    double X[9], Y[9], Z[9];
-    X[0] = X[1] = Y[0] = Y[1] = Z[0] = Z[1] = 0.0;
-    X[2] = Y[2] = Z[2] = 1.0;
-#pragma unroll
-    for (int i = 3; i < 9; ++i) {
-      X[i] = X[i - 1] * x;
-      Y[i] = Y[i - 1] * y;
-      Z[i] = Z[i - 1] * z;
-    }
-    for (int j = 0; j < nc; ++j) {
-      double q[NQ];
-#pragma unroll
-      for (int i = 0; i < NQ; ++i) q[i] = 0.0;
-      const int tb = c_comp_off[sg.type][j], te = c_comp_off[sg.type][j + 1];
-      for (int t = tb; t < te; ++t) {
-        const Term T = c_terms[t];
-        const int a = T.a, b = T.b, c = T.z;
-        const double X0 = X[a + 2], Y0 = Y[b + 2], Z0 = Z[c + 2];
-        q[0] += T.c * X0 * Y0 * Z0 * R0;
-        if (DERIV >= 1) {
-          const double Xa = a * X[a + 1], Xb = X[a + 3];
-          const double Ya = b * Y[b + 1], Yb = Y[b + 3];
-          const double Za = c * Z[c + 1], Zb = Z[c + 3];
-          q[1] += T.c * Y0 * Z0 * (Xa * R0 - 2.0 * Xb * R1);
-          q[2] += T.c * X0 * Z0 * (Ya * R0 - 2.0 * Yb * R1);
-          q[3] += T.c * X0 * Y0 * (Za * R0 - 2.0 * Zb * R1);
-          if (DERIV >= 2) {
-            const double Xaa = a * (a - 1) * X[a], Xd = X[a + 4];
-            const double Yaa = b * (b - 1) * Y[b], Yd = Y[b + 4];
-            const double Zaa = c * (c - 1) * Z[c], Zd = Z[c + 4];
-            q[4] += T.c * Y0 * Z0 * (Xaa * R0 - 2.0 * (2 * a + 1) * X0 * R1 + 4.0 * Xd * R2);
-            q[5] += T.c * Z0 * (Xa * Ya * R0 - 2.0 * (Xa * Yb + Xb * Ya) * R1 + 4.0 * Xb * Yb * R2);
-            q[6] += T.c * Y0 * (Xa * Za * R0 - 2.0 * (Xa * Zb + Xb * Za) * R1 + 4.0 * Xb * Zb * R2);
-            q[7] += T.c * X0 * Z0 * (Yaa * R0 - 2.0 * (2 * b + 1) * Y0 * R1 + 4.0 * Yd * R2);
-            q[8] += T.c * X0 * (Ya * Za * R0 - 2.0 * (Ya * Zb + Yb * Za) * R1 + 4.0 * Yb * Zb * R2);
-            q[9] += T.c * X0 * Y0 * (Zaa * R0 - 2.0 * (2 * c + 1) * Z0 * R1 + 4.0 * Zd * R2);
-          }
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < NQ; ++i)
-        if (i < nq_out) o[i * ld_q + j] = q[i];
-    }
+    eval_segment<DERIV>(sg, alpha, coef, px, py, pz, out + p * ld_point + sg.ao0, ld_q, nq_out);
+  }
+}
+
+// One CTA per tile: (significant segment, point) pairs, segment index
+// fastest so that consecutive threads write consecutive AO columns.  Padding
+// columns [ktrue, kt) are zeroed.
+template <int DERIV>
+__global__ void __launch_bounds__(kAoThreads)
+    ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
+                   const double* __restrict__ coef, TileBatch tb) {
+  const int t = blockIdx.x;
+  const int ns = tb.nsig[t], TP = tb.TP;
+  const int32_t* sl = tb.segs + (int64_t)t * nseg;
+  const int32_t* k0 = tb.k0 + (int64_t)t * nseg;
+  const double* xyz = tb.xyz + (int64_t)t * TP * 3;
+  double* A = tb.ao + (int64_t)t * tb.nq * TP * tb.Kcap;
+  const int64_t ld_q = (int64_t)TP * tb.Kcap;
+  const int total = ns * TP;
+  for (int idx = threadIdx.x; idx < total; idx += kAoThreads) {
+    const int i = idx % ns, j = idx / ns;
+    const DevSeg sg = segs[sl[i]];
+    eval_segment<DERIV>(sg, alpha, coef, xyz[3 * j], xyz[3 * j + 1], xyz[3 * j + 2],
+                        A + (int64_t)j * tb.Kcap + k0[i], ld_q, tb.nq);
+  }
+  const int kt_true = tb.ktrue[t], kt = tb.kt[t];
+  const int npad = kt - kt_true;
+  for (int idx = threadIdx.x; idx < tb.nq * TP * npad; idx += kAoThreads) {
+    const int c = idx % npad, r = idx / npad;  // r = q * TP + j
+    A[(int64_t)r * tb.Kcap + kt_true + c] = 0.0;
   }
 }
 
@@ -150,6 +191,17 @@ static int launch_ao_impl(const ctc_molecule* mol, const PointSrc& src, int64_t 
 int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
               int nq_out, int ld, cudaStream_t st) {
   return launch_ao_impl(mol, src, n, deriv, out, nq_out, (int64_t)nq_out * ld, ld, st);
+}
+
+int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cudaStream_t st) {
+  if (tb.C <= 0) return CTC_OK;
+  switch (deriv) {
+    case 0: ao_tile_kernel<0><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb); break;
+    case 1: ao_tile_kernel<1><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb); break;
+    default: ao_tile_kernel<2><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb);
+  }
+  CTC_CUDA_TRY(cudaGetLastError());
+  return CTC_OK;
 }
 
 // Public layout (nq, n, M).

@@ -87,6 +87,26 @@ struct Scratch {
 // ESP pair data built once per molecule (see ctc_esp.cu).
 struct EspTables;
 
+// One chunk of point tiles of the screened local pipeline (device pointers).
+// A tile holds TP points; its significant segments, compacted, define the
+// tile's own K dimension (kt, padded to a multiple of 64).
+struct TileBatch {
+  int C = 0;          // tiles in this chunk
+  int TP = 0;         // points per tile (32 or 128)
+  int Kcap = 0;       // capacity of the compact K dimension (>= Mpad)
+  int nq = 0;         // AO quantities per point (1, 4, 10)
+  double* xyz = nullptr;    // [C][TP][3]
+  int64_t* out = nullptr;   // [C][TP] output index, -1 for padding
+  int32_t* nsig = nullptr;  // [C] significant segments
+  int32_t* ktrue = nullptr; // [C] compact AOs before padding
+  int32_t* kt = nullptr;    // [C] compact AOs padded to 64
+  int32_t* segs = nullptr;  // [C][nseg] significant segment ids
+  int32_t* k0 = nullptr;    // [C][nseg] compact offset of each significant segment
+  int32_t* aomap = nullptr; // [C][Kcap] compact -> AO index, -1 for padding
+  double* ao = nullptr;     // [C][nq][TP][Kcap] AO values and derivatives
+};
+constexpr int kKtAlign = 64;
+
 }  // namespace ctc
 
 struct ctc_molecule {
@@ -120,6 +140,8 @@ struct ctc_molecule {
 namespace ctc {
 
 // ---- kernels / launchers (ctc_ao.cu) ----
+// AO block of every tile of a batch on its significant segments only.
+int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cudaStream_t st);
 int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
               int nq_out, int ld, cudaStream_t st);
 // AO output in (nq, n, M) layout for ctc_eval_ao.
@@ -138,14 +160,15 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
 
 // ---- tensor-core split path (ctc_tc.cu) ----
 int prepare_tc(ctc_molecule* mol, cudaStream_t st);
-int tc_local_chunk(ctc_molecule* mol, const LocalPlan& plan, const double* ao, int64_t n,
-                   int64_t out_offset, const ctc_params* prm, const ctc_outputs* out,
-                   cudaStream_t st);
+int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
+                   const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
 
 // ---- FP64 path (ctc_local.cu) ----
-int fp64_local_chunk(ctc_molecule* mol, const LocalPlan& plan, const double* ao, int64_t n,
-                     int64_t out_offset, const ctc_params* prm, const ctc_outputs* out,
-                     cudaStream_t st);
+int fp64_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
+                     const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
+
+// per-point finalisation shared by the contraction kernels (ctc_local.cu)
+struct LocalSums;
 
 // ---- ESP (ctc_esp.cu) ----
 int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, cudaStream_t st);

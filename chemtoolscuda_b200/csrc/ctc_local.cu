@@ -10,13 +10,25 @@
 //     rho     = sum_nu G0 phi                     grad_k = 2 sum_nu G0 d_k phi
 //     H_ij    = 2 [sum_nu Gi d_j phi + sum_nu G0 d_i d_j phi]
 //     lap     = tr H                              tau_PD = 1/2 sum_k sum_nu Gk d_k phi
-// so one pass computes the AO block of a chunk of points, then one kernel per
-// chunk forms the G tiles and reduces them against the AO values in its
-// epilogue: G never leaves the SM and each point's descriptors are finished
-// in registers.  The FP64 contraction runs on the double-precision matrix
-// units (mma.sync m8n8k4 f64); the tensor-core split form is in ctc_tc.cu.
+//
+// Screening.  An AO contributes only where its shell reaches: on the
+// 200-atom benchmark molecule ~9% of the AOs exceed 1e-14 at a typical grid
+// point.  Points are therefore grouped into spatially compact tiles (3-D
+// blocks of a cubic grid, or runs of Morton-sorted points), every tile builds
+// its own list of significant segments (distance from the tile's bounding
+// sphere below the segment's screening radius, where every AO value and
+// derivative has dropped below 1e-18), and the contraction of that tile runs
+// over its compacted AO set only: G_t = A_t D[S_t, S_t] with D gathered from
+// L2 by index.  The AOs left out are below 1e-18 on the whole tile.
+//
+// Per chunk of tiles: screen -> AO block (compact) -> contraction + epilogue.
+// The FP64 contraction runs on the double-precision matrix units (mma.sync
+// m8n8k4 f64); the tensor-core split form is in ctc_tc.cu.
 #include <algorithm>
 #include <cmath>
+
+#include <cub/block/block_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include "ctc_internal.h"
 
@@ -36,6 +48,19 @@ LocalPlan plan_local(const ctc_outputs* o) {
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
+
+__device__ __forceinline__ int ncomp_of_type_dev(int type) {
+  switch (type) {
+    case 0: return 1;
+    case 1: return 3;
+    case 2: return 6;
+    case 3: return 5;
+    case 4: return 10;
+    case 5: return 7;
+    case 6: return 15;
+    default: return 9;
+  }
+}
 
 // Per-point partial sums produced by the contraction epilogues:
 //   s[0] rho, s[1..3] sum G0 d_k phi, s[4..9] Hb_ij = sum G0 d_i d_j phi,
@@ -89,6 +114,156 @@ __device__ __forceinline__ void finalize_point(const double* s, int nqa, int nq_
   if (o.general_ked) o.general_ked[idx] = tau + 0.25 * (prm.ked_a - 1.0) * lap;
 }
 
+// ------------------------------------------------------------------ tiles
+constexpr int kTileThreads = 256;
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void morton_kernel(const double* __restrict__ pts, int64_t n, double lox, double loy,
+                              double loz, double inv_cell, uint32_t* keys, int32_t* vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  auto q = [&](double v, double lo) {
+    double c = (v - lo) * inv_cell;
+    c = c < 0.0 ? 0.0 : (c > 1023.0 ? 1023.0 : c);
+    return (uint32_t)c;
+  };
+  keys[i] = spread10(q(pts[3 * i], lox)) | (spread10(q(pts[3 * i + 1], loy)) << 1) |
+            (spread10(q(pts[3 * i + 2], loz)) << 2);
+  vals[i] = (int32_t)i;
+}
+
+// Tiles of TP consecutive sorted points; padding slots repeat the tile's first point.
+__global__ void tile_gather_kernel(const double* __restrict__ pts, const int32_t* __restrict__ perm,
+                                   int64_t n, int64_t t0, TileBatch tb) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)tb.C * tb.TP) return;
+  const int64_t t = gid / tb.TP;
+  const int j = (int)(gid % tb.TP);
+  const int64_t g = (t0 + t) * tb.TP + j;
+  const bool v = g < n;
+  const int64_t p = perm[v ? g : (t0 + t) * tb.TP];
+  tb.xyz[3 * gid] = pts[3 * p];
+  tb.xyz[3 * gid + 1] = pts[3 * p + 1];
+  tb.xyz[3 * gid + 2] = pts[3 * p + 2];
+  tb.out[gid] = v ? p : -1;
+}
+
+// Cubic grid: tile = TX x TY x TZ block of grid points (z fastest).
+__global__ void tile_cubic_kernel(PointSrc src, int nx, int TX, int TY, int TZ, int nby, int nbz,
+                                  int64_t t0, TileBatch tb) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)tb.C * tb.TP) return;
+  const int64_t t = t0 + gid / tb.TP;
+  const int j = (int)(gid % tb.TP);
+  const int64_t bz = t % nbz, by = (t / nbz) % nby, bx = t / ((int64_t)nbz * nby);
+  const int iz = j % TZ, iy = (j / TZ) % TY, ix = j / (TZ * TY);
+  int64_t i = bx * TX + ix, k = by * TY + iy, l = bz * TZ + iz;
+  const bool v = i < nx && k < src.ny && l < src.nz;
+  if (!v) { i = bx * TX; k = by * TY; l = bz * TZ; }
+  const double fi = (double)i, fj = (double)k, fk = (double)l;
+  tb.xyz[3 * gid] = src.o[0] + fi * src.ax[0] + fj * src.ax[3] + fk * src.ax[6];
+  tb.xyz[3 * gid + 1] = src.o[1] + fi * src.ax[1] + fj * src.ax[4] + fk * src.ax[7];
+  tb.xyz[3 * gid + 2] = src.o[2] + fi * src.ax[2] + fj * src.ax[5] + fk * src.ax[8];
+  tb.out[gid] = v ? (i * src.ny + k) * (int64_t)src.nz + l : -1;
+}
+
+// One CTA per tile: bounding sphere of the tile's points, then the ordered
+// list of segments whose screening sphere meets it.
+__global__ void __launch_bounds__(kTileThreads)
+    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb) {
+  using Scan = cub::BlockScan<int, kTileThreads>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ double red[3][kTileThreads / 32];
+  __shared__ double sctr[3], srad;
+  __shared__ int base_s, base_k;
+  const int t = blockIdx.x, TP = tb.TP;
+  const double* xyz = tb.xyz + (int64_t)t * TP * 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // centre = mean of the tile's points (padding repeats a real point)
+  double c[3] = {0, 0, 0};
+  for (int j = threadIdx.x; j < TP; j += kTileThreads)
+    for (int d = 0; d < 3; ++d) c[d] += xyz[3 * j + d];
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) c[d] += __shfl_xor_sync(0xffffffffu, c[d], o);
+    if (lane == 0) red[d][warp] = c[d];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double acc = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) acc += red[threadIdx.x][w];
+    sctr[threadIdx.x] = acc / TP;
+  }
+  __syncthreads();
+  double r2 = 0.0;
+  for (int j = threadIdx.x; j < TP; j += kTileThreads) {
+    const double dx = xyz[3 * j] - sctr[0], dy = xyz[3 * j + 1] - sctr[1], dz = xyz[3 * j + 2] - sctr[2];
+    r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+  }
+  for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+  if (lane == 0) red[0][warp] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) m = fmax(m, red[0][w]);
+    srad = sqrt(m) * (1.0 + 1e-12) + 1e-9;
+    base_s = 0;
+    base_k = 0;
+  }
+  __syncthreads();
+  const double rad = srad;
+  int32_t* sl = tb.segs + (int64_t)t * nseg;
+  int32_t* k0 = tb.k0 + (int64_t)t * nseg;
+  int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+  for (int s0 = 0; s0 < nseg; s0 += kTileThreads) {
+    const int s = s0 + threadIdx.x;
+    int sig = 0, nc = 0;
+    DevSeg sg;
+    if (s < nseg) {
+      sg = segs[s];
+      const double dx = sg.cx - sctr[0], dy = sg.cy - sctr[1], dz = sg.cz - sctr[2];
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      const double lim = sqrt(sg.rcut2) + rad;
+      if (d <= lim) {
+        sig = 1;
+        nc = ncomp_of_type_dev(sg.type);
+      }
+    }
+    // pack (segment count, AO count) into one int: both sums stay below 2^16
+    int packed, ptot;
+    Scan(scan_tmp).ExclusiveSum((sig << 16) | nc, packed, ptot);
+    const int2 pos = make_int2(packed >> 16, packed & 0xffff);
+    const int2 tot = make_int2(ptot >> 16, ptot & 0xffff);
+    if (sig) {
+      const int ks = base_k + pos.y;
+      sl[base_s + pos.x] = s;
+      k0[base_s + pos.x] = ks;
+      for (int q = 0; q < nc; ++q) am[ks + q] = sg.ao0 + q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      base_s += tot.x;
+      base_k += tot.y;
+    }
+    __syncthreads();
+  }
+  const int kt_true = base_k;
+  const int kt = (kt_true + kKtAlign - 1) / kKtAlign * kKtAlign;
+  for (int k = kt_true + threadIdx.x; k < kt; k += kTileThreads) am[k] = -1;
+  if (threadIdx.x == 0) {
+    tb.nsig[t] = base_s;
+    tb.ktrue[t] = kt_true;
+    tb.kt[t] = kt;
+  }
+}
+
 // ------------------------------------------------------------------ FP64 contraction kernel
 constexpr int BM = 128, BN = 64, BK = 32, STAGES = 3;
 constexpr int A_LD = BK + 4;  // 36 doubles: conflict-free fragment loads
@@ -99,11 +274,17 @@ constexpr int kThreads = 256;
 constexpr size_t kSmemPipe = sizeof(double) * STAGES * (A_STAGE + B_STAGE);
 constexpr size_t kSmemC = sizeof(double) * BM * C_LD;
 constexpr size_t kSmemFp64 = kSmemPipe > kSmemC ? kSmemPipe : kSmemC;
+static_assert(kKtAlign % BN == 0 && kKtAlign % BK == 0, "tile K alignment");
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   int sz = valid ? 16 : 0;
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -117,15 +298,15 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-// One CTA owns PTS = 128/NQA points; tile row r holds quantity r / PTS of
-// point r % PTS (quantity 0 = phi, 1..3 = d_k phi).  It sweeps all nu tiles
-// of 64 columns, each with a full K loop over mu, and reduces every finished
-// G tile against the AO values of its columns.
+// One CTA per tile of PTS = 128/NQA points; tile row r holds quantity r / PTS
+// of point r % PTS (quantity 0 = phi, 1..3 = d_k phi).  It sweeps the tile's
+// compact nu range in 64-column slices, each with a full K loop over the
+// compact mu range (B = D gathered by index), and reduces every finished G
+// slice against the AO values of its columns.
 template <int NQA>
 __global__ void __launch_bounds__(kThreads)
-    fp64_local_kernel(const double* __restrict__ ao, int nq_ao, int ld,
-                      const double* __restrict__ D, int Mpad, int64_t n, ctc_outputs out,
-                      int64_t out_off, ctc_params prm) {
+    fp64_tile_kernel(TileBatch tb, const double* __restrict__ D, int Mpad, ctc_outputs out,
+                     ctc_params prm) {
   constexpr int PTS = BM / NQA;
   constexpr int TPP = kThreads / PTS;  // epilogue threads per point
   constexpr int NS = NQA == 4 ? 16 : 4;
@@ -133,20 +314,26 @@ __global__ void __launch_bounds__(kThreads)
   double* sA = smem;
   double* sB = smem + STAGES * A_STAGE;
   double* sC = smem;  // aliases the pipeline after the K loop
+  __shared__ int s_colmap[BN];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp & 3, wn = warp >> 2;
-  const int64_t p0 = (int64_t)blockIdx.x * PTS;
+  const int t = blockIdx.x;
+  const int kt = tb.kt[t];
+  const int nq_ao = tb.nq;
+  const int64_t ldq = (int64_t)PTS * tb.Kcap;  // stride between quantities
+  const double* A = tb.ao + (int64_t)t * nq_ao * ldq;
+  const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
 
-  // epilogue ownership
   const int epl = tid / TPP, esub = tid % TPP;
-  const int64_t ep = p0 + epl;
   double acc_s[NS];
 #pragma unroll
   for (int i = 0; i < NS; ++i) acc_s[i] = 0.0;
 
-  const int nkb = Mpad / BK;
-  for (int n0 = 0; n0 < Mpad; n0 += BN) {
+  const int nkb = kt / BK;
+  for (int n0 = 0; n0 < kt; n0 += BN) {
+    if (tid < BN) s_colmap[tid] = am[n0 + tid];
+    __syncthreads();
     double c[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -157,23 +344,21 @@ __global__ void __launch_bounds__(kThreads)
       double* a = sA + stage * A_STAGE;
       double* b = sB + stage * B_STAGE;
       const int k0 = kb * BK;
-      // A: 128 rows x 32 doubles = 2048 chunks of 16 B, 8 per thread
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        int ch = tid + i * kThreads;
-        int r = ch >> 4, cc = (ch & 15) * 2;
-        int q = r / PTS, pl = r % PTS;
-        int64_t p = p0 + pl;
-        bool v = p < n;
-        const double* src = ao + ((v ? p : 0) * nq_ao + q) * (int64_t)ld + k0 + cc;
-        cp_async16(a + r * A_LD + cc, src, v);
+        const int ch = tid + i * kThreads;
+        const int r = ch >> 4, cc = (ch & 15) * 2;
+        const int q = r / PTS, pl = r % PTS;
+        cp_async16(a + r * A_LD + cc, A + q * ldq + (int64_t)pl * tb.Kcap + k0 + cc, true);
       }
-      // B: 32 rows (k) x 64 doubles = 1024 chunks, 4 per thread
+      // B gather: 32 rows (compact mu) x 64 columns (compact nu), 8 bytes each
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        int ch = tid + i * kThreads;
-        int r = ch >> 5, cc = (ch & 31) * 2;
-        cp_async16(b + r * B_LD + cc, D + (int64_t)(k0 + r) * Mpad + n0 + cc, true);
+      for (int i = 0; i < 8; ++i) {
+        const int e = tid + i * kThreads;
+        const int r = e >> 6, cc = e & 63;
+        const int mu = am[k0 + r], nu = s_colmap[cc];
+        const bool v = mu >= 0 && nu >= 0;
+        cp_async8(b + r * B_LD + cc, D + (v ? (int64_t)mu * Mpad + nu : 0), v);
       }
     };
 
@@ -206,29 +391,28 @@ __global__ void __launch_bounds__(kThreads)
     }
     cp_async_wait<0>();
     __syncthreads();
-    // stage the G tile
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        int r = wm * 32 + i * 8 + (lane >> 2);
-        int cc = wn * 32 + j * 8 + 2 * (lane & 3);
+        const int r = wm * 32 + i * 8 + (lane >> 2);
+        const int cc = wn * 32 + j * 8 + 2 * (lane & 3);
         sC[r * C_LD + cc] = c[i][j][0];
         sC[r * C_LD + cc + 1] = c[i][j][1];
       }
     __syncthreads();
-    if (ep < n) {
-      const double* aop = ao + ep * (int64_t)nq_ao * ld + n0;
+    {
+      const double* aop = A + (int64_t)epl * tb.Kcap + n0;
       for (int v = esub; v < BN; v += TPP) {
         const double G0 = sC[(0 * PTS + epl) * C_LD + v];
         const double phi = aop[v];
         acc_s[0] += G0 * phi;
         if (nq_ao >= 4) {
-          const double d0 = aop[ld + v], d1 = aop[2 * ld + v], d2 = aop[3 * ld + v];
+          const double d0 = aop[ldq + v], d1 = aop[2 * ldq + v], d2 = aop[3 * ldq + v];
           acc_s[1] += G0 * d0;
           acc_s[2] += G0 * d1;
           acc_s[3] += G0 * d2;
-          if (NQA == 4) {
+          if constexpr (NQA == 4) {
             const double G1 = sC[(1 * PTS + epl) * C_LD + v];
             const double G2 = sC[(2 * PTS + epl) * C_LD + v];
             const double G3 = sC[(3 * PTS + epl) * C_LD + v];
@@ -240,7 +424,7 @@ __global__ void __launch_bounds__(kThreads)
             acc_s[15] += G3 * d2;
             if (nq_ao == 10) {
 #pragma unroll
-              for (int h = 0; h < 6; ++h) acc_s[4 + h] += G0 * aop[(4 + h) * ld + v];
+              for (int h = 0; h < 6; ++h) acc_s[4 + h] += G0 * aop[(4 + h) * ldq + v];
             }
           }
         }
@@ -248,80 +432,177 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
   }
-  // reduce the TPP partial sums of each point (consecutive lanes)
 #pragma unroll
   for (int i = 0; i < NS; ++i)
 #pragma unroll
     for (int off = TPP / 2; off > 0; off >>= 1)
       acc_s[i] += __shfl_xor_sync(0xffffffffu, acc_s[i], off);
-  if (esub == 0 && ep < n) {
+  const int64_t oidx = tb.out[(int64_t)t * PTS + epl];
+  if (esub == 0 && oidx >= 0) {
     double s[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) s[i] = i < NS ? acc_s[i] : 0.0;
-    finalize_point(s, NQA, nq_ao, out, out_off + ep, prm);
+    finalize_point(s, NQA, nq_ao, out, oidx, prm);
   }
 }
 
 }  // namespace
 
-int fp64_local_chunk(ctc_molecule* mol, const LocalPlan& plan, const double* ao, int64_t n,
-                     int64_t out_off, const ctc_params* prm, const ctc_outputs* out,
-                     cudaStream_t st) {
-  if (n <= 0) return CTC_OK;
+int fp64_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
+                     const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
+  if (tb.C <= 0) return CTC_OK;
   static bool attr_set[2] = {false, false};
   if (plan.nqa == 4) {
     if (!attr_set[1]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_local_kernel<4>,
+      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<4>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
       attr_set[1] = true;
     }
-    int64_t grid = (n + (BM / 4) - 1) / (BM / 4);
-    fp64_local_kernel<4><<<(unsigned)grid, kThreads, kSmemFp64, st>>>(
-        ao, plan.nq_ao, mol->Mpad, mol->d_D, mol->Mpad, n, *out, out_off, *prm);
+    fp64_tile_kernel<4><<<tb.C, kThreads, kSmemFp64, st>>>(tb, mol->d_D, mol->Mpad, *out, *prm);
   } else {
     if (!attr_set[0]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_local_kernel<1>,
+      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<1>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
       attr_set[0] = true;
     }
-    int64_t grid = (n + BM - 1) / BM;
-    fp64_local_kernel<1><<<(unsigned)grid, kThreads, kSmemFp64, st>>>(
-        ao, plan.nq_ao, mol->Mpad, mol->d_D, mol->Mpad, n, *out, out_off, *prm);
+    fp64_tile_kernel<1><<<tb.C, kThreads, kSmemFp64, st>>>(tb, mol->d_D, mol->Mpad, *out, *prm);
   }
   CTC_CUDA_TRY(cudaGetLastError());
   return CTC_OK;
 }
 
-int eval_local(ctc_molecule* mol, const PointSrc& src0, int64_t n, int precision,
+// ------------------------------------------------------------------ driver
+namespace {
+
+struct Carve {
+  char* p;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) / 256 * 256;
+    T* r = (T*)(p + off);
+    off += sizeof(T) * count;
+    return r;
+  }
+};
+
+size_t tile_bytes(const ctc_molecule* mol, int C, int TP) {
+  const size_t Kcap = mol->Mpad;
+  size_t b = 0;
+  auto add = [&](size_t x) { b = (b + 255) / 256 * 256 + x; };
+  add(sizeof(double) * C * TP * 3);
+  add(sizeof(int64_t) * C * TP);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * (size_t)C * mol->nseg);
+  add(sizeof(int32_t) * (size_t)C * mol->nseg);
+  add(sizeof(int32_t) * (size_t)C * Kcap);
+  return b + 256;
+}
+
+}  // namespace
+
+int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
                const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
   if (n < 0) return fail(CTC_ERR_INVALID, "eval_local: negative point count");
   if (n == 0) return CTC_OK;
   if (precision != CTC_PREC_FP64 && precision != CTC_PREC_TC_SPLIT)
     return fail(CTC_ERR_INVALID, "eval_local: unknown precision " + std::to_string(precision));
+  if (!src.cubic && n > (int64_t)INT32_MAX)
+    return fail(CTC_ERR_INVALID, "eval_local: at most 2^31-1 points per call");
   const LocalPlan plan = plan_local(out);
   if (precision == CTC_PREC_TC_SPLIT) {
     int rc = prepare_tc(mol, st);
     if (rc != CTC_OK) return rc;
   }
-  const int64_t chunk = std::min<int64_t>(chunk_points(mol, plan.nq_ao), n);
-  const size_t ao_bytes = sizeof(double) * (size_t)chunk * plan.nq_ao * mol->Mpad;
-  int rc = mol->ws_ao.ensure(ao_bytes, st);
-  if (rc != CTC_OK) return rc;
-  double* ao = (double*)mol->ws_ao.p;
-  for (int64_t c0 = 0; c0 < n; c0 += chunk) {
-    const int64_t nc = std::min(chunk, n - c0);
-    PointSrc src = src0;
-    src.offset += c0;
-    if (mol->Mpad > mol->M) {
-      CTC_CUDA_TRY(cudaMemset2DAsync(ao + mol->M, sizeof(double) * mol->Mpad, 0,
-                                     sizeof(double) * (mol->Mpad - mol->M), nc * plan.nq_ao, st));
+  const int TP = 128 / plan.nqa;
+  int TX = 2, TY = 4, TZ = 4;
+  if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
+  int64_t ntiles, nbx = 0, nby = 0, nbz = 0;
+  int nx = 0;
+  if (src.cubic) {
+    nx = (int)(n / ((int64_t)src.ny * src.nz));
+    nbx = (nx + TX - 1) / TX;
+    nby = (src.ny + TY - 1) / TY;
+    nbz = (src.nz + TZ - 1) / TZ;
+    ntiles = nbx * nby * nbz;
+  } else {
+    ntiles = (n + TP - 1) / TP;
+  }
+  // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within ~2 GB
+  const size_t ao_per_tile = sizeof(double) * (size_t)plan.nq_ao * TP * mol->Mpad;
+  int64_t C = std::max<int64_t>(148, (int64_t)(((size_t)2 << 30) / ao_per_tile));
+  C = std::min<int64_t>(C, ntiles);
+  int rc;
+  if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;
+  if ((rc = mol->ws_misc.ensure(tile_bytes(mol, (int)C, TP), st)) != CTC_OK) return rc;
+  TileBatch tb;
+  tb.TP = TP;
+  tb.Kcap = mol->Mpad;
+  tb.nq = plan.nq_ao;
+  tb.ao = (double*)mol->ws_ao.p;
+  {
+    Carve cv{(char*)mol->ws_misc.p};
+    tb.xyz = cv.take<double>((size_t)C * TP * 3);
+    tb.out = cv.take<int64_t>((size_t)C * TP);
+    tb.nsig = cv.take<int32_t>(C);
+    tb.ktrue = cv.take<int32_t>(C);
+    tb.kt = cv.take<int32_t>(C);
+    tb.segs = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.k0 = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.aomap = cv.take<int32_t>((size_t)C * tb.Kcap);
+  }
+  // explicit points: Morton order over the molecule's box padded by 12 bohr
+  int32_t* perm = nullptr;
+  if (!src.cubic) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int a = 0; a < mol->natom; ++a)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], mol->atom_xyz[3 * a + d]);
+        hi[d] = std::max(hi[d], mol->atom_xyz[3 * a + d]);
+      }
+    if (mol->natom == 0)
+      for (int d = 0; d < 3; ++d) { lo[d] = -1; hi[d] = 1; }
+    double ext = 0;
+    for (int d = 0; d < 3; ++d) {
+      lo[d] -= 12.0;
+      hi[d] += 12.0;
+      ext = std::max(ext, hi[d] - lo[d]);
     }
-    rc = launch_ao(mol, src, nc, plan.deriv, ao, plan.nq_ao, mol->Mpad, st);
-    if (rc != CTC_OK) return rc;
-    if (precision == CTC_PREC_FP64)
-      rc = fp64_local_chunk(mol, plan, ao, nc, c0, prm, out, st);
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 30, st);
+    const size_t need = 4 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
+    if ((rc = mol->ws_part.ensure(need, st)) != CTC_OK) return rc;
+    Carve cv{(char*)mol->ws_part.p};
+    uint32_t* k_in = cv.take<uint32_t>(n);
+    uint32_t* k_out = cv.take<uint32_t>(n);
+    int32_t* v_in = cv.take<int32_t>(n);
+    perm = cv.take<int32_t>(n);
+    void* tmp = cv.take<char>(tmp_bytes);
+    morton_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src.pts, n, lo[0], lo[1], lo[2],
+                                                                1024.0 / ext, k_in, v_in);
+    CTC_CUDA_TRY(cudaGetLastError());
+    CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
+                                                 30, st));
+  }
+  for (int64_t t0 = 0; t0 < ntiles; t0 += C) {
+    tb.C = (int)std::min<int64_t>(C, ntiles - t0);
+    const int64_t npts = (int64_t)tb.C * TP;
+    const unsigned g = (unsigned)((npts + 255) / 256);
+    if (src.cubic)
+      tile_cubic_kernel<<<g, 256, 0, st>>>(src, nx, TX, TY, TZ, (int)nby, (int)nbz, t0, tb);
     else
-      rc = tc_local_chunk(mol, plan, ao, nc, c0, prm, out, st);
+      tile_gather_kernel<<<g, 256, 0, st>>>(src.pts, perm, n, t0, tb);
+    CTC_CUDA_TRY(cudaGetLastError());
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb);
+    CTC_CUDA_TRY(cudaGetLastError());
+    if ((rc = launch_ao_tiles(mol, tb, plan.deriv, st)) != CTC_OK) return rc;
+    if (precision == CTC_PREC_FP64)
+      rc = fp64_local_tiles(mol, plan, tb, prm, out, st);
+    else
+      rc = tc_local_tiles(mol, plan, tb, prm, out, st);
     if (rc != CTC_OK) return rc;
   }
   return CTC_OK;
