@@ -605,6 +605,8 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
       rc = tc_local_tiles(mol, plan, tb, prm, out, st);
     if (rc != CTC_OK) return rc;
   }
+  // the tensor-core kernels report bounded-wait timeouts through the status word
+  if (precision == CTC_PREC_TC_SPLIT) return check_status(mol, st, "tensor-core contraction");
   return CTC_OK;
 }
 
