@@ -1,0 +1,527 @@
+#!/usr/bin/env python
+"""Benchmark: grid points/s for all local density descriptors on one B200 (or N).
+
+Workload (one step): the 200-atom synthetic molecule of the second benchmark
+configuration (pure d and f shells, ~2 650 basis functions, D = 2 C C^T with
+400 occupied orthonormal columns) evaluated on a 215^3 cubic grid at 0.2 bohr
+(9 938 375 points) for rho, grad rho, Hessian, Laplacian, tau_PD,
+tau_alpha (alpha = 0.5) and the reduced density gradient, with the contraction
+on the tensor-core split path (INT8 tcgen05, exact int32 accumulation, FP64
+epilogue).  Inputs are synthetic (seeded); there is no dataset.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision tc|fp64]
+    python bench.py --impl reference ...   # the reference's own CUDA drivers
+
+Prints one JSON line.  For N > 1 run under torch.distributed.run: every rank
+evaluates its own full-size grid (an independent density matrix of the same
+molecule), so per-GPU work is fixed ("scaling": "weak") and nothing crosses
+GPUs except the barrier and the max-over-ranks timing reduction.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from chemtoolscuda_b200 import synthetic as S  # noqa: E402
+
+SHAPE = (215, 215, 215)
+SPACING = 0.2
+KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg")
+WIDTH = dict(rho=1, grad=3, hess=9, lap=1, tau_pd=1, tau_alpha=1, rdg=1, shannon=1, weizsacker=1,
+             thomas_fermi=1, gge=1, general_ked=1)
+OUT_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon", "weizsacker",
+            "thomas_fermi", "gge", "general_ked")
+METRIC = "grid pts/s for rho, grad rho, Hessian, lap rho, tau_PD, tau_alpha, RDG (TC split vs FP64 form)"
+ALPHA = 0.5
+
+
+class Outputs(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in OUT_KEYS]
+
+
+class Params(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("gge_a", C.c_double), ("gge_b", C.c_double),
+                ("ked_a", C.c_double)]
+
+
+class Basis(C.Structure):
+    _fields_ = [("nshell", C.c_int32), ("centers", C.c_void_p), ("shell_atom", C.c_void_p),
+                ("nprim", C.c_void_p), ("nseg", C.c_void_p), ("angmoms", C.c_void_p),
+                ("exps", C.c_void_p), ("coeffs", C.c_void_p)]
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------- distributed plumbing
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 8:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------- library handle
+def load_lib():
+    lib = C.CDLL(os.path.join(ROOT, "chemtoolscuda_b200", "libchemtools_cuda.so"))
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    lib.ctc_last_error.restype = C.c_char_p
+    lib.ctc_molecule_create.argtypes = [vp, i32, vp, vp, vp, i32, vp]
+    lib.ctc_molecule_destroy.argtypes = [vp]
+    lib.ctc_molecule_prepare.argtypes = [vp, i32]
+    lib.ctc_eval_cubic.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp]
+    lib.ctc_eval_local_host.argtypes = [vp, vp, i64, i32, vp, vp]
+    lib.ctc_eval_esp.argtypes = [vp, vp, i64, vp, vp]
+    lib.ctc_molecule_get_stats.argtypes = [vp, vp]
+    lib.ctc_molecule_reset_stats.argtypes = [vp]
+    lib.ctc_molecule_set_profiling.argtypes = [vp, i32]
+    return lib
+
+
+def check(lib, rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib.ctc_last_error().decode()}")
+
+
+def create(lib, mol):
+    f = mol.flat()
+    keep = {k: np.ascontiguousarray(v) for k, v in f.items()}
+    keep["coords"] = np.ascontiguousarray(mol.coords)
+    keep["charges"] = np.ascontiguousarray(mol.charges)
+    keep["D"] = np.ascontiguousarray(mol.D)
+    b = Basis(len(keep["nprim"]), keep["centers"].ctypes.data, keep["shell_atom"].ctypes.data,
+              keep["nprim"].ctypes.data, keep["nseg"].ctypes.data, keep["angmoms"].ctypes.data,
+              keep["exps"].ctypes.data, keep["coeffs"].ctypes.data)
+    h = C.c_void_p()
+    check(lib, lib.ctc_molecule_create(C.byref(b), len(mol.coords), keep["coords"].ctypes.data,
+                                       keep["charges"].ctypes.data, keep["D"].ctypes.data,
+                                       keep["D"].shape[0], C.byref(h)), "create")
+    return h
+
+
+def stats(lib, h):
+    s = (C.c_double * 8)()
+    check(lib, lib.ctc_molecule_get_stats(h, s), "stats")
+    return list(s)
+
+
+# --------------------------------------------------------------------------- peaks
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def int8_peak_tops():
+    """Dense INT8 tensor throughput measured here with cuBLASLt (torch._int_mm), best of 5."""
+    import torch
+    try:
+        n = 8192
+        a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12, "measured (cuBLASLt int8 8192^3, burst)"
+    except Exception as ex:  # pragma: no cover
+        pk, src = measured_peaks()
+        return 2.0 * pk["bf16_tflops"], f"2 x {src} bf16 ({ex.__class__.__name__})"
+
+
+def fp64_peak_tflops():
+    """Dense FP64 throughput measured here with cuBLAS (torch.matmul float64), best of 5."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def profile_traffic(name):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get(name)
+    return None
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args, ws, rank, local):
+    import torch
+    lib = load_lib()
+    mol = S.make_molecule("c2", seed=0)
+    if rank > 0:
+        # independent density matrix per rank (same molecule and grid structure)
+        rng = np.random.default_rng(1000 + rank)
+        mol.D = S.make_density_matrix(rng, mol.nbasis, 400)
+    h = create(lib, mol)
+    prec = 1 if args.precision == "tc" else 0
+    check(lib, lib.ctc_molecule_prepare(h, prec), "prepare")
+    shape = tuple(args.shape)
+    origin, axes = S.cube_grid(mol, SPACING, shape)
+    n = int(np.prod(shape))
+    outs = {k: torch.empty(n * WIDTH[k], dtype=torch.float64, device="cuda") for k in KEYS}
+    o = Outputs(**{k: outs[k].data_ptr() for k in KEYS})
+    prm = Params(ALPHA, 1 / 9, 1 / 6, 1.0)
+    org = np.ascontiguousarray(origin)
+    ax = np.ascontiguousarray(axes)
+    sh = np.ascontiguousarray(np.array(shape, dtype=np.int32))
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step(p=prec):
+        check(lib, lib.ctc_eval_cubic(h, org.ctypes.data, ax.ctypes.data, sh.ctypes.data, p,
+                                      C.byref(prm), C.byref(o), stream), "eval_cubic")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    check(lib, lib.ctc_molecule_reset_stats(h), "reset")
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            step()
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = allreduce_max(ms, ws)
+    st = stats(lib, h)
+    clocks = clk.summary()
+    value = ws * n * args.steps / (ms_max * 1e-3)
+
+    # dominant kernel, timed live with events on the launching stream (separate pass)
+    check(lib, lib.ctc_molecule_reset_stats(h), "reset")
+    check(lib, lib.ctc_molecule_set_profiling(h, 1), "profiling")
+    step()
+    torch.cuda.synchronize()
+    pst = stats(lib, h)
+    check(lib, lib.ctc_molecule_set_profiling(h, 0), "profiling")
+    macs = pst[3]                      # sum over tiles of rows * kt^2
+    kern_ms = pst[6]
+    result = None
+    if rank == 0:
+        if prec == 1:
+            peak, peak_src = int8_peak_tops()
+            achieved = 26.0 * macs / (kern_ms * 1e-3) / 1e12      # 13 int8 products x 2 ops
+            roof = {"kernel": "tc_tile_kernel (tcgen05.mma kind::i8)", "bound": "tensor",
+                    "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
+                    "frac": achieved / peak, "peak_source": peak_src,
+                    "fp64_equiv_tflops": 2.0 * macs / (kern_ms * 1e-3) / 1e12,
+                    "kernel_ms_per_step": kern_ms, "ao_kernel_ms_per_step": pst[7],
+                    "traffic": profile_traffic("tc_tile_kernel")}
+        else:
+            peak = fp64_peak_tflops()
+            achieved = 2.0 * macs / (kern_ms * 1e-3) / 1e12
+            roof = {"kernel": "fp64_tile_kernel (mma.sync m8n8k4 f64)", "bound": "tensor",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s (fp64)",
+                    "frac": achieved / peak, "peak_source": "measured (cuBLAS DGEMM 8192^3)",
+                    "kernel_ms_per_step": kern_ms, "ao_kernel_ms_per_step": pst[7],
+                    "traffic": profile_traffic("fp64_tile_kernel")}
+        result = dict(value=value, ms=ms_max / args.steps, stats=st, roof=roof, clocks=clocks, n=n)
+
+    # FP64 form of the same step (the metric compares the two forms)
+    fp64 = None
+    if prec == 1 and not args.no_fp64_form:
+        step(0)
+        torch.cuda.synchronize()
+        barrier(ws)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step(0)
+        e1.record()
+        torch.cuda.synchronize()
+        fms = allreduce_max(e0.elapsed_time(e1), ws)
+        fp64 = {"value": ws * n / (fms * 1e-3), "ms_per_step": fms, "steps": 1}
+
+    # end to end through the C ABI with host buffers (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        pts = S.cube_points(origin, axes, shape)
+        hout = {k: np.empty(n * WIDTH[k]) for k in KEYS}
+        ho = Outputs(**{k: hout[k].ctypes.data for k in KEYS})
+        check(lib, lib.ctc_eval_local_host(h, pts.ctypes.data, n, prec, C.byref(prm), C.byref(ho)), "e2e")
+        ksteps = max(1, min(args.steps, 3))
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(ksteps):
+            check(lib, lib.ctc_eval_local_host(h, pts.ctypes.data, n, prec, C.byref(prm),
+                                               C.byref(ho)), "e2e")
+        el = allreduce_max(time.perf_counter() - t0, ws)
+        e2e = {"value": ws * n * ksteps / el, "unit": "grid points/s", "steps": ksteps,
+               "h2d_bytes_per_step": int(pts.nbytes),
+               "d2h_bytes_per_step": int(sum(v.nbytes for v in hout.values())),
+               "api": "ctc_eval_local_host (C ABI, host buffers)"}
+
+    # ESP throughput (metric's second part): 100-atom molecule, surface points sample
+    esp = None
+    if rank == 0 and not args.no_esp:
+        mol5 = S.make_molecule("c5", seed=0)
+        h5 = create(lib, mol5)
+        sp = S.surface_points(mol5, seed=0)
+        m = min(len(sp), args.esp_points)
+        p5 = torch.as_tensor(np.ascontiguousarray(sp[:m]), device="cuda")
+        o5 = torch.empty(m, dtype=torch.float64, device="cuda")
+        check(lib, lib.ctc_eval_esp(h5, p5.data_ptr(), m, o5.data_ptr(), stream), "esp")
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        check(lib, lib.ctc_eval_esp(h5, p5.data_ptr(), m, o5.data_ptr(), stream), "esp")
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        esp = {"value": m / (ems * 1e-3), "unit": "ESP points/s", "points": m,
+               "surface_points_total": int(len(sp)), "nbasis": mol5.nbasis, "atoms": 100}
+        lib.ctc_molecule_destroy(h5)
+
+    # CPU baseline: the FP64 oracle on this host's cores, bounded sample of the same grid
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        rng = np.random.default_rng(7)
+        allp = S.cube_points(origin, axes, shape)
+        sample = allp[rng.choice(n, args.cpu_points, replace=False)]
+        t0 = time.perf_counter()
+        O.eval_local(mol.flat(), mol.D, sample, alpha=ALPHA,
+                     keys=("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg"))
+        el = time.perf_counter() - t0
+        cpu = {"value": args.cpu_points / el, "unit": "grid points/s", "cores": os.cpu_count(),
+               "kind": "port", "sample": f"{args.cpu_points} random points of the 215^3 grid, "
+                                          "all seven descriptors, FP64 C++/OpenMP oracle"}
+    lib.ctc_molecule_destroy(h)
+    return result, fp64, e2e, esp, cpu, mol.nbasis
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return None
+    libp = os.path.join(ROOT, "oracle", "_ref", "libctc_ref.so")
+    if not os.path.exists(libp):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libctc_ref.so not built (make -C oracle ref)"}
+    lib = C.CDLL(libp)
+    vp, i32, dbl = C.c_void_p, C.c_int, C.c_double
+    lib.ref_create.restype = vp
+    lib.ref_create.argtypes = [i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, i32]
+    lib.ref_last_error.restype = C.c_char_p
+    for f in ("density", "gradient", "hessian", "laplacian", "tau_pd", "rdg"):
+        getattr(lib, "ref_" + f).argtypes = [vp, vp, i32, vp]
+    lib.ref_tau_general.argtypes = [vp, vp, i32, dbl, vp]
+    mol = S.make_molecule("c2", seed=0)
+    f = mol.flat()
+    keep = [np.ascontiguousarray(f[k]) for k in ("centers", "nprim", "nseg", "angmoms", "exps", "coeffs")]
+    xyz, chg, D = np.ascontiguousarray(mol.coords), np.ascontiguousarray(mol.charges), np.ascontiguousarray(mol.D)
+    h = lib.ref_create(len(f["nprim"]), *[k.ctypes.data for k in keep], len(xyz), xyz.ctypes.data,
+                       chg.ctypes.data, D.ctypes.data, D.shape[0])
+    if not h:
+        return {"impl": "reference", "unavailable": lib.ref_last_error().decode()}
+    shape = tuple(args.shape)
+    origin, axes = S.cube_grid(mol, SPACING, shape)
+    allp = S.cube_points(origin, axes, shape)
+    n = args.ref_points
+    rng = np.random.default_rng(11)
+    M = mol.nbasis
+    # the reference indexes with 32-bit integers: keep 6 * M * n below 2^31
+    assert 6 * M * n < 2 ** 31
+
+    def step(pts):
+        outs = {"density": np.empty(n), "gradient": np.empty((n, 3)), "hessian": np.empty((n, 3, 3)),
+                "laplacian": np.empty(n), "tau_pd": np.empty(n), "rdg": np.empty(n)}
+        for k, a in outs.items():
+            rc = getattr(lib, "ref_" + k)(h, pts.ctypes.data, n, a.ctypes.data)
+            if rc != 0:
+                raise RuntimeError(f"reference {k}: {lib.ref_last_error().decode()}")
+        ta = np.empty(n)
+        if lib.ref_tau_general(h, pts.ctypes.data, n, ALPHA, ta.ctypes.data) != 0:
+            raise RuntimeError(lib.ref_last_error().decode())
+
+    samples = [np.ascontiguousarray(allp[rng.choice(len(allp), n, replace=False)])
+               for _ in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        step(samples[i])
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(samples[args.warmup + i])
+    el = time.perf_counter() - t0
+    value = n * args.steps / el
+    return {"metric": METRIC, "value": value, "unit": "grid points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "c2: 200-atom molecule, 215^3 grid at 0.2 bohr, all local descriptors",
+                       "nbasis": M, "points_per_step": n,
+                       "reference_calls": "evaluate_electron_density_on_any_grid, _gradient, _hessian, "
+                                          "evaluate_laplacian, evaluate_positive_definite_kinetic_density, "
+                                          "evaluate_general_kinetic_energy_density, compute_reduced_density_gradient"},
+            "cpu_baseline": {"value": value, "unit": "grid points/s", "cores": 1, "kind": "reference",
+                             "sample": f"{n} random points of the 215^3 grid per step; the reference is "
+                                       "CUDA code (no CPU implementation): its own drivers built from "
+                                       "its sources for sm_100a (oracle/_ref) run on this box's GPU"},
+            "e2e": {"value": value, "unit": "grid points/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="tc", choices=["tc", "fp64"])
+    ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-esp", action="store_true")
+    ap.add_argument("--no-fp64-form", action="store_true")
+    ap.add_argument("--cpu-points", type=int, default=1500)
+    ap.add_argument("--esp-points", type=int, default=20000)
+    ap.add_argument("--ref-points", type=int, default=16384)
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        line = run_reference(args, ws, rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+    res, fp64, e2e, esp, cpu, nbasis = run_ours(args, ws, rank, local)
+    if rank == 0:
+        dtype = ("int8x4 split operands, exact int32 accumulation, fp64 AO/epilogue"
+                 if args.precision == "tc" else "f64")
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "grid points/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic",
+            "config": {"workload": "c2: 200-atom molecule (pure d/f), 215^3 cubic grid at 0.2 bohr, "
+                                   "rho+grad+Hessian+lap+tau_PD+tau_alpha(0.5)+RDG",
+                       "nbasis": nbasis, "points_per_gpu": res["n"], "precision": args.precision,
+                       "l2": "outputs of one step (1.35 GB) exceed L2; basis tables and D stay L2-resident by design",
+                       "tiles_per_step": res["stats"][0] / args.steps,
+                       "mean_compact_aos_per_tile": res["stats"][2] / max(res["stats"][0], 1)},
+            "roofline": res["roof"], "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(res["stats"][4]), "clocks": res["clocks"],
+            "fp64_form": fp64, "esp": esp,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

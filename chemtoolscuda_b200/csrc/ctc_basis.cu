@@ -124,6 +124,16 @@ static double screening_radius2(const std::vector<double>& a, const std::vector<
 
 using namespace ctc;
 
+static void clear_prof(ctc_molecule* m) {
+  for (int k = 0; k < 2; ++k) {
+    for (auto& pr : m->prof_ev[k]) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    m->prof_ev[k].clear();
+  }
+}
+
 extern "C" {
 
 const char* ctc_last_error(void) { return g_last_error.c_str(); }
@@ -242,7 +252,9 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
   ALLOC_COPY(m->d_D, Dpad.data(), MM);
 #undef ALLOC_COPY
   if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
-      cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess) {
+      cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess ||
+      cudaMalloc((void**)&m->d_stats, sizeof(double) * 8) != cudaSuccess ||
+      cudaMemset(m->d_stats, 0, sizeof(double) * 8) != cudaSuccess) {
     ctc_molecule_destroy(m);
     return fail(CTC_ERR_NOMEM, "status word allocation failed");
   }
@@ -253,6 +265,7 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
 int ctc_molecule_destroy(ctc_molecule* m) {
   if (!m) return CTC_OK;
   cudaDeviceSynchronize();
+  clear_prof(m);
   destroy_esp(m);
   cudaFree(m->d_segs);
   cudaFree(m->d_alpha);
@@ -263,6 +276,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   cudaFree(m->d_Dsl);
   cudaFree(m->d_Dscale);
   cudaFree(m->d_status);
+  cudaFree(m->d_stats);
   m->ws_ao.release();
   m->ws_sl.release();
   m->ws_part.release();
@@ -299,6 +313,45 @@ int ctc_molecule_set_coordinates(ctc_molecule* m, const double* xyz) {
   CTC_CUDA_TRY(cudaMemcpy(m->d_segs, m->segs.data(), sizeof(DevSeg) * m->segs.size(),
                           cudaMemcpyHostToDevice));
   m->esp_valid = false;
+  return CTC_OK;
+}
+
+int ctc_molecule_get_stats(ctc_molecule* m, double* stats) {
+  if (!m || !stats) return fail(CTC_ERR_INVALID, "get_stats: null argument");
+  double d[8] = {0};
+  CTC_CUDA_TRY(cudaDeviceSynchronize());
+  CTC_CUDA_TRY(cudaMemcpy(d, m->d_stats, sizeof(double) * 8, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < 8; ++i) stats[i] = 0.0;
+  stats[0] = d[0];
+  stats[1] = d[1];
+  stats[2] = d[2];
+  stats[3] = d[3];
+  stats[4] = m->host_launches;
+  stats[5] = m->host_chunks;
+  for (int k = 0; k < 2; ++k) {
+    double ms_total = 0.0;
+    for (auto& pr : m->prof_ev[k]) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ms_total += ms;
+    }
+    stats[6 + k] = ms_total;
+  }
+  return CTC_OK;
+}
+
+int ctc_molecule_set_profiling(ctc_molecule* m, int32_t on) {
+  if (!m) return fail(CTC_ERR_INVALID, "set_profiling: null molecule");
+  m->prof = on != 0;
+  return CTC_OK;
+}
+
+int ctc_molecule_reset_stats(ctc_molecule* m) {
+  if (!m) return fail(CTC_ERR_INVALID, "reset_stats: null molecule");
+  CTC_CUDA_TRY(cudaDeviceSynchronize());
+  CTC_CUDA_TRY(cudaMemset(m->d_stats, 0, sizeof(double) * 8));
+  m->host_launches = 0;
+  m->host_chunks = 0;
+  clear_prof(m);
   return CTC_OK;
 }
 

@@ -131,6 +131,12 @@ struct ctc_molecule {
   bool dsl_valid = false;
   // per-call status word written by kernels
   int32_t* d_status = nullptr;
+  // work counters: [0] tiles [1] points [2] sum kt_true [3] sum rows*kt^2 (device, doubles)
+  double* d_stats = nullptr;
+  double host_launches = 0, host_chunks = 0;
+  // optional kernel timing: event pairs of contraction (0) and AO (1) kernels
+  bool prof = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[2];
   // scratch
   ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc;
   ctc::EspTables* esp = nullptr;
@@ -183,5 +189,23 @@ int64_t chunk_points(const ctc_molecule* mol, int nq_ao);
 
 // status word helpers
 int check_status(ctc_molecule* mol, cudaStream_t st, const char* what);
+
+// Records a start/stop event pair around a launch when profiling is on.
+struct ProfScope {
+  ctc_molecule* mol;
+  int kind;
+  cudaStream_t st;
+  cudaEvent_t b = nullptr, e = nullptr;
+  ProfScope(ctc_molecule* m, int k, cudaStream_t s) : mol(m), kind(k), st(s) {
+    if (mol->prof && cudaEventCreate(&b) == cudaSuccess && cudaEventCreate(&e) == cudaSuccess)
+      cudaEventRecord(b, st);
+  }
+  ~ProfScope() {
+    if (b && e) {
+      cudaEventRecord(e, st);
+      mol->prof_ev[kind].push_back({b, e});
+    }
+  }
+};
 
 }  // namespace ctc

@@ -178,7 +178,8 @@ __global__ void tile_cubic_kernel(PointSrc src, int nx, int TX, int TY, int TZ, 
 // One CTA per tile: bounding sphere of the tile's points, then the ordered
 // list of segments whose screening sphere meets it.
 __global__ void __launch_bounds__(kTileThreads)
-    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb) {
+    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb, int rows,
+                  double* __restrict__ stats) {
   using Scan = cub::BlockScan<int, kTileThreads>;
   __shared__ typename Scan::TempStorage scan_tmp;
   __shared__ double red[3][kTileThreads / 32];
@@ -261,6 +262,12 @@ __global__ void __launch_bounds__(kTileThreads)
     tb.nsig[t] = base_s;
     tb.ktrue[t] = kt_true;
     tb.kt[t] = kt;
+    int npts = 0;
+    for (int j = 0; j < TP; ++j) npts += tb.out[(int64_t)t * TP + j] >= 0;
+    atomicAdd(&stats[0], 1.0);
+    atomicAdd(&stats[1], (double)npts);
+    atomicAdd(&stats[2], (double)kt_true);
+    atomicAdd(&stats[3], (double)rows * (double)kt * (double)kt);
   }
 }
 
@@ -530,9 +537,10 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
   } else {
     ntiles = (n + TP - 1) / TP;
   }
-  // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within ~2 GB
+  // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within ~6 GB,
+  // at least one full wave of CTAs on 148 SMs
   const size_t ao_per_tile = sizeof(double) * (size_t)plan.nq_ao * TP * mol->Mpad;
-  int64_t C = std::max<int64_t>(148, (int64_t)(((size_t)2 << 30) / ao_per_tile));
+  int64_t C = std::max<int64_t>(148, (int64_t)(((size_t)6 << 30) / ao_per_tile));
   C = std::min<int64_t>(C, ntiles);
   int rc;
   if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;
@@ -596,15 +604,24 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
     else
       tile_gather_kernel<<<g, 256, 0, st>>>(src.pts, perm, n, t0, tb);
     CTC_CUDA_TRY(cudaGetLastError());
-    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb);
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, 128, mol->d_stats);
     CTC_CUDA_TRY(cudaGetLastError());
-    if ((rc = launch_ao_tiles(mol, tb, plan.deriv, st)) != CTC_OK) return rc;
-    if (precision == CTC_PREC_FP64)
+    {
+      ProfScope ps(mol, 1, st);
+      if ((rc = launch_ao_tiles(mol, tb, plan.deriv, st)) != CTC_OK) return rc;
+    }
+    if (precision == CTC_PREC_FP64) {
+      ProfScope ps(mol, 0, st);
       rc = fp64_local_tiles(mol, plan, tb, prm, out, st);
-    else
+    } else {
       rc = tc_local_tiles(mol, plan, tb, prm, out, st);
+    }
     if (rc != CTC_OK) return rc;
+    // tile points, screen, AO block, contraction (+ operand slicing on the tensor-core path)
+    mol->host_launches += precision == CTC_PREC_FP64 ? 4 : 5;
+    mol->host_chunks += 1;
   }
+  if (!src.cubic) mol->host_launches += 2;  // Morton keys + radix sort
   // the tensor-core kernels report bounded-wait timeouts through the status word
   if (precision == CTC_PREC_TC_SPLIT) return check_status(mol, st, "tensor-core contraction");
   return CTC_OK;

@@ -588,6 +588,7 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   a.prm = *prm;
   a.status = mol->d_status;
   static bool attr[2] = {false, false};
+  ProfScope ps(mol, 0, st);
   if (plan.nqa == 4) {
     if (!attr[1]) {
       CTC_CUDA_TRY(cudaFuncSetAttribute(tc_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc));

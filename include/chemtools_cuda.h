@@ -161,6 +161,20 @@ int ctc_eval_esp_host(ctc_molecule* mol, const double* h_points, int64_t npoints
 int ctc_adjoint(ctc_molecule* mol, const double* d_points, int64_t npoints, const double* d_v_rho,
                 const double* d_v_grad, double* d_dLdD, double* d_dLdR, void* stream);
 
+/* ---- diagnostics ---------------------------------------------------------------------------- */
+
+/* Work counters of the local-descriptor pipeline accumulated since the last
+ * reset (no counterpart in the reference): stats[0] tiles, [1] points in
+ * tiles, [2] sum of compact AO counts, [3] sum over tiles of rows * kt^2
+ * (multiply-adds of the contraction on the screened AO set), [4] kernel
+ * launches issued, [5] chunks, [6] milliseconds spent in the contraction
+ * kernels and [7] in the AO kernels (both 0 unless profiling is on).
+ * Synchronises the device. */
+int ctc_molecule_get_stats(ctc_molecule* mol, double* stats /* [8] */);
+int ctc_molecule_reset_stats(ctc_molecule* mol);
+/* Time the contraction and AO kernels with CUDA events on their stream. */
+int ctc_molecule_set_profiling(ctc_molecule* mol, int32_t on);
+
 /* ---- misc ---------------------------------------------------------------------------------- */
 const char* ctc_last_error(void);
 const char* ctc_version(void);
