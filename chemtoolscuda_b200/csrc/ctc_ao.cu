@@ -128,26 +128,95 @@ __global__ void __launch_bounds__(kAoThreads)
   }
 }
 
-// One CTA per tile: (significant segment, point) pairs, segment index
-// fastest so that consecutive threads write consecutive AO columns.  Padding
-// columns [ktrue, kt) are zeroed.
+#include "ctc_ao_poly.inc"
+
+// Type-specialised evaluation of one segment at one point: the polynomial
+// code of every component has literal exponents (ctc_ao_poly.inc), so the
+// powers stay in registers.  Same arithmetic as eval_segment.
+template <int DERIV, int TYPE>
+__device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __restrict__ alpha,
+                                           const double* __restrict__ coef, double px, double py,
+                                           double pz, double* __restrict__ o, int64_t ld_q,
+                                           int nq_out) {
+  constexpr int L = TYPE == 0 ? 0 : (TYPE == 1 ? 1 : (TYPE <= 3 ? 2 : (TYPE <= 5 ? 3 : 4)));
+  constexpr int NC = TYPE == 0 ? 1 : TYPE == 1 ? 3 : TYPE == 2 ? 6 : TYPE == 3 ? 5
+                     : TYPE == 4 ? 10 : TYPE == 5 ? 7 : TYPE == 6 ? 15 : 9;
+  constexpr int NP = L + 5;  // powers x^(i-2) for i < NP
+  const double x = px - sg.cx, y = py - sg.cy, z = pz - sg.cz;
+  const double r2 = x * x + y * y + z * z;
+  if (r2 > sg.rcut2) {
+    for (int q = 0; q < nq_out; ++q)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) o[q * ld_q + j] = 0.0;
+    return;
+  }
+  double R0 = 0.0, R1 = 0.0, R2 = 0.0;
+  for (int k = 0; k < sg.nprim; ++k) {
+    const double a = alpha[sg.prim0 + k];
+    const double e = coef[sg.prim0 + k] * exp(-a * r2);
+    R0 += e;
+    if (DERIV >= 1) R1 += a * e;
+    if (DERIV >= 2) R2 += a * a * e;
+  }
+  double X[NP], Y[NP], Z[NP];
+  X[0] = X[1] = Y[0] = Y[1] = Z[0] = Z[1] = 0.0;
+  X[2] = Y[2] = Z[2] = 1.0;
+#pragma unroll
+  for (int i = 3; i < NP; ++i) {
+    X[i] = X[i - 1] * x;
+    Y[i] = Y[i - 1] * y;
+    Z[i] = Z[i - 1] * z;
+  }
+  if constexpr (TYPE == 0) ao_poly_0<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 1) ao_poly_1<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 2) ao_poly_2<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 3) ao_poly_3<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 4) ao_poly_4<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 5) ao_poly_5<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else if constexpr (TYPE == 6) ao_poly_6<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  else ao_poly_7<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+}
+
+template <int DERIV>
+__device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __restrict__ alpha,
+                                              const double* __restrict__ coef, double px, double py,
+                                              double pz, double* __restrict__ o, int64_t ld_q,
+                                              int nq_out) {
+  switch (sg.type) {
+    case 0: eval_typed<DERIV, 0>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 1: eval_typed<DERIV, 1>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 2: eval_typed<DERIV, 2>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 3: eval_typed<DERIV, 3>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 4: eval_typed<DERIV, 4>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 5: eval_typed<DERIV, 5>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 6: eval_typed<DERIV, 6>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    default: eval_typed<DERIV, 7>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+  }
+}
+
+// One CTA per tile; each warp takes one significant segment at a time and
+// its lanes take the tile's points, so a warp always runs one segment type.
+// Padding columns [ktrue, kt) are zeroed.
 template <int DERIV>
 __global__ void __launch_bounds__(kAoThreads)
     ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
                    const double* __restrict__ coef, TileBatch tb) {
   const int t = blockIdx.x;
   const int ns = tb.nsig[t], TP = tb.TP;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t* sl = tb.segs + (int64_t)t * nseg;
   const int32_t* k0 = tb.k0 + (int64_t)t * nseg;
   const double* xyz = tb.xyz + (int64_t)t * TP * 3;
   double* A = tb.ao + (int64_t)t * tb.nq * TP * tb.Kcap;
   const int64_t ld_q = (int64_t)TP * tb.Kcap;
-  const int total = ns * TP;
-  for (int idx = threadIdx.x; idx < total; idx += kAoThreads) {
-    const int i = idx % ns, j = idx / ns;
-    const DevSeg sg = segs[sl[i]];
-    eval_segment<DERIV>(sg, alpha, coef, xyz[3 * j], xyz[3 * j + 1], xyz[3 * j + 2],
-                        A + (int64_t)j * tb.Kcap + k0[i], ld_q, tb.nq);
+  for (int pg = 0; pg < TP; pg += 32) {
+    const int j = pg + lane;
+    const double px = xyz[3 * j], py = xyz[3 * j + 1], pz = xyz[3 * j + 2];
+    double* row = A + (int64_t)j * tb.Kcap;
+    for (int i = warp; i < ns; i += kAoThreads / 32) {
+      const DevSeg sg = segs[sl[i]];
+      eval_dispatch<DERIV>(sg, alpha, coef, px, py, pz, row + k0[i], ld_q, tb.nq);
+    }
   }
   const int kt_true = tb.ktrue[t], kt = tb.kt[t];
   const int npad = kt - kt_true;

@@ -26,6 +26,7 @@
 // m8n8k4 f64); the tensor-core split form is in ctc_tc.cu.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
@@ -540,7 +541,12 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
   // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within ~6 GB,
   // at least one full wave of CTAs on 148 SMs
   const size_t ao_per_tile = sizeof(double) * (size_t)plan.nq_ao * TP * mol->Mpad;
-  int64_t C = std::max<int64_t>(148, (int64_t)(((size_t)6 << 30) / ao_per_tile));
+  size_t budget = (size_t)6 << 30;
+  if (const char* env = std::getenv("CTC_CHUNK_BYTES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) budget = (size_t)v;
+  }
+  int64_t C = std::max<int64_t>(148, (int64_t)(budget / ao_per_tile));
   C = std::min<int64_t>(C, ntiles);
   int rc;
   if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;

@@ -266,6 +266,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   __shared__ uint32_t tmem_base_sh;
   __shared__ int s_abort;
   __shared__ double s_sums[32][16];
+  __shared__ double s_cscale[2][kN];
 
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
@@ -301,38 +302,48 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 
   if (warp < 4) {
     // ---------------- producers
+    // Thread tid owns the 4 mu columns k4 = (tid % 16) * 4 of every stage and the
+    // 8 nu rows n = tid / 16 + 8 i of every nu tile, so its AO indices are
+    // loaded once per stage / tile and its 32 gathers of D are independent.
     const int tid = threadIdx.x;
+    const int k4 = (tid & 15) * 4, nrow0 = tid >> 4;
     int it = 0;
     for (int nt = 0; nt < nnt && !s_abort; ++nt) {
       const int n0 = nt * kN;
+      int nu[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int nc = n0 + nrow0 + 8 * i;
+        nu[i] = nc < kt ? am[nc] : -1;
+      }
       for (int kb = 0; kb < nkb; ++kb, ++it) {
         const int s = it % kStages;
         const uint32_t ph = (it / kStages) & 1;
-        if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
         const int k0 = kb * kBK;
+        int mu[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mu[j] = am[k0 + k4 + j];
+        uint32_t w[8][4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            w[i][j] = (nu[i] >= 0 && mu[j] >= 0) ? __ldg(args.Dp + (int64_t)nu[i] * args.Mpad + mu[j]) : 0u;
+        if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
         if (tid == 0) {
           mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
           for (int p = 0; p < kPlanes; ++p)
             tma_load_2d(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0, (t * kPlanes + p) * kRows,
                         &full_bar[s]);
         }
-        // B gather: 64 nu rows x 16 words (4 mu each)
         uint8_t* b = sB + s * kBStageBytes;
-        for (int u = tid; u < kN * (kBK / 4); u += 128) {
-          const int n = u / (kBK / 4), k4 = (u % (kBK / 4)) * 4;
-          const int nc = n0 + n;
-          const int nu = nc < kt ? am[nc] : -1;
-          uint32_t w[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int mu = am[k0 + k4 + i];
-            w[i] = (nu >= 0 && mu >= 0) ? args.Dp[(int64_t)nu * args.Mpad + mu] : 0u;
-          }
-          const uint32_t off = sw64_offset(n, k4);
+        for (int i = 0; i < 8; ++i) {
+          const uint32_t off = sw64_offset(nrow0 + 8 * i, k4);
 #pragma unroll
           for (int p = 0; p < kPlanes; ++p) {
-            const uint32_t v = ((w[0] >> (8 * p)) & 255) | (((w[1] >> (8 * p)) & 255) << 8) |
-                               (((w[2] >> (8 * p)) & 255) << 16) | (((w[3] >> (8 * p)) & 255) << 24);
+            const uint32_t v = ((w[i][0] >> (8 * p)) & 255) | (((w[i][1] >> (8 * p)) & 255) << 8) |
+                               (((w[i][2] >> (8 * p)) & 255) << 16) | (((w[i][3] >> (8 * p)) & 255) << 24);
             *(uint32_t*)(b + p * kBPlaneBytes + off) = v;
           }
         }
@@ -385,19 +396,30 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     // ---------------- epilogue (warps 5..8 -> TMEM lane quarters 1,2,3,0)
     const int quarter = warp & 3;
     const int r = quarter * 32 + lane;
+    const int etid = (warp - 5) * 32 + lane;  // 0..127
     constexpr int PTS = kRows / NQA;
     const int q = r / PTS, pl = r % PTS;
     const int nq_ao = tb.nq;
     const int64_t ldq = (int64_t)tb.TP * tb.Kcap;
     const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + (int64_t)pl * tb.Kcap;
     const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 60);
+    // quantities this row is reduced against: q = 0 -> phi, d phi, d2 phi; q = k -> d_j phi, j >= k
+    const int qa = (q == 0) ? 0 : q;
+    const int qb = (q == 0) ? nq_ao : 4;
     double sums[10];
 #pragma unroll
     for (int i = 0; i < 10; ++i) sums[i] = 0.0;
     for (int nt = 0; nt < nnt && !s_abort; ++nt) {
+      const int n0 = nt * kN;
+      double* cs = s_cscale[nt & 1];
+      if (etid < kN) {
+        const int nc = n0 + etid;
+        const int nu = nc < kt ? am[nc] : -1;
+        cs[etid] = nu >= 0 ? ldexp(1.0, args.fexp[nu]) : 0.0;
+      }
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");
       if (!mbar_wait(&tfull_bar, nt & 1)) { s_abort = 1; break; }
       tc_fence_after();
-      const int n0 = nt * kN;
 #pragma unroll 1
       for (int c = 0; c < kN / 16; ++c) {
         double g[16];
@@ -412,28 +434,18 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 #pragma unroll
           for (int j = 0; j < 16; ++j) g[j] += (double)v[j] * w;
         }
-#pragma unroll 4
-        for (int j = 0; j < 16; ++j) {
-          const int nc = n0 + c * 16 + j;
-          if (nc >= kt) break;
-          const int nu = am[nc];
-          if (nu < 0) continue;
-          const double G = g[j] * rowscale * ldexp(1.0, args.fexp[nu]);
-          if (q == 0) {
-            sums[0] += G * aop[nc];
-            if (nq_ao >= 4) {
-              sums[1] += G * aop[ldq + nc];
-              sums[2] += G * aop[2 * ldq + nc];
-              sums[3] += G * aop[3 * ldq + nc];
-              if (nq_ao == 10) {
 #pragma unroll
-                for (int h = 0; h < 6; ++h) sums[4 + h] += G * aop[(4 + h) * ldq + nc];
-              }
-            }
-          } else {
-            // G_q row (q = 1, 2, 3): Ha_{q j} for j >= q
-            for (int jj = q; jj <= 3; ++jj) sums[jj - q] += G * aop[jj * ldq + nc];
-          }
+        for (int j = 0; j < 16; ++j) g[j] *= rowscale * cs[c * 16 + j];
+        const int col = n0 + c * 16;
+        for (int qq = qa; qq < qb; ++qq) {
+          const double2* src = reinterpret_cast<const double2*>(aop + qq * ldq + col);
+          double2 v2[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) v2[j] = __ldg(src + j);
+          double acc = 0.0;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc += g[2 * j] * v2[j].x + g[2 * j + 1] * v2[j].y;
+          sums[qq - qa] += acc;
         }
       }
       tc_fence_before();
