@@ -1,0 +1,627 @@
+// ctc_tiles.cuh -- the screened point-tile pipeline shared by the local
+// descriptors (ctc_local.cu) and the adjoint (ctc_adjoint.cu).
+//
+// Points are grouped into spatially compact tiles (3-D blocks of a cubic grid,
+// or runs of Morton-sorted points); every tile lists the segments whose
+// screening sphere (every AO value and derivative below 1e-18 outside it)
+// meets the tile's bounding sphere, and works on that compacted AO set only.
+// Per chunk of tiles: tile points -> screen -> AO block (compact) -> a
+// contraction kernel supplied by the caller.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <functional>
+
+#include <cub/block/block_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
+
+#include "ctc_internal.h"
+
+namespace ctc {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+__device__ __forceinline__ int ncomp_of_type_dev(int type) {
+  switch (type) {
+    case 0: return 1;
+    case 1: return 3;
+    case 2: return 6;
+    case 3: return 5;
+    case 4: return 10;
+    case 5: return 7;
+    case 6: return 15;
+    default: return 9;
+  }
+}
+
+// Per-point partial sums produced by the contraction epilogues:
+//   s[0] rho, s[1..3] sum G0 d_k phi, s[4..9] Hb_ij = sum G0 d_i d_j phi,
+//   s[10..15] Ha_ij = sum Gi d_j phi  (ij = xx xy xz yy yz zz)
+__device__ __forceinline__ void finalize_point(const double* s, int nqa, int nq_ao,
+                                               const ctc_outputs& o, int64_t idx,
+                                               const ctc_params& prm) {
+  const double rho = s[0];
+  const double g0 = 2.0 * s[1], g1 = 2.0 * s[2], g2 = 2.0 * s[3];
+  double H[6] = {0, 0, 0, 0, 0, 0};
+  double tau = 0.0;
+  if (nqa == 4) {
+    for (int i = 0; i < 6; ++i) H[i] = 2.0 * (s[10 + i] + (nq_ao == 10 ? s[4 + i] : 0.0));
+    tau = 0.5 * (s[10] + s[13] + s[15]);
+  }
+  const double lap = H[0] + H[3] + H[5];
+  if (o.rho) o.rho[idx] = rho;
+  if (o.grad) {
+    o.grad[3 * idx] = g0;
+    o.grad[3 * idx + 1] = g1;
+    o.grad[3 * idx + 2] = g2;
+  }
+  if (o.hess) {
+    double* h = o.hess + 9 * idx;
+    h[0] = H[0]; h[1] = H[1]; h[2] = H[2];
+    h[3] = H[1]; h[4] = H[3]; h[5] = H[4];
+    h[6] = H[2]; h[7] = H[4]; h[8] = H[5];
+  }
+  if (o.lap) o.lap[idx] = lap;
+  if (o.tau_pd) o.tau_pd[idx] = tau;
+  if (o.tau_alpha) o.tau_alpha[idx] = tau + prm.alpha * lap;
+  const double gsq = g0 * g0 + g1 * g1 + g2 * g2;
+  if (o.rdg) {
+    // s = 1/(2 (3 pi^2)^(1/3)) |grad rho| / rho^(4/3), ratio set to 1e-20 where
+    // rho^(4/3) <= 1e-20 (src/evaluate_densbased.cu:44-89, src/cuda_utils.cu:71-84)
+    const double pref = 0.5 / cbrt(3.0 * kPi * kPi);
+    const double d43 = pow(rho, 4.0 / 3.0);
+    const double q = d43 > 1e-20 ? sqrt(gsq) / d43 : 1e-20;
+    o.rdg[idx] = pref * q;
+  }
+  if (o.shannon) o.shannon[idx] = rho * log(rho);
+  double w = 0.0, tf = 0.0;
+  if (o.weizsacker || o.gge) {
+    const double den = 8.0 * rho;
+    w = den > 1e-20 ? gsq / den : 1e-20;
+  }
+  if (o.thomas_fermi || o.gge) tf = 0.3 * pow(3.0 * kPi * kPi, 2.0 / 3.0) * pow(rho, 5.0 / 3.0);
+  if (o.weizsacker) o.weizsacker[idx] = w;
+  if (o.thomas_fermi) o.thomas_fermi[idx] = tf;
+  if (o.gge) o.gge[idx] = tf + prm.gge_a * w + prm.gge_b * lap;
+  if (o.general_ked) o.general_ked[idx] = tau + 0.25 * (prm.ked_a - 1.0) * lap;
+}
+
+// ------------------------------------------------------------------ tiles
+constexpr int kTileThreads = 256;
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void morton_kernel(const double* __restrict__ pts, int64_t n, double lox, double loy,
+                              double loz, double inv_cell, uint32_t* keys, int32_t* vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  auto q = [&](double v, double lo) {
+    double c = (v - lo) * inv_cell;
+    c = c < 0.0 ? 0.0 : (c > 1023.0 ? 1023.0 : c);
+    return (uint32_t)c;
+  };
+  keys[i] = spread10(q(pts[3 * i], lox)) | (spread10(q(pts[3 * i + 1], loy)) << 1) |
+            (spread10(q(pts[3 * i + 2], loz)) << 2);
+  vals[i] = (int32_t)i;
+}
+
+// Tiles of TP consecutive sorted points; padding slots repeat the tile's first point.
+__global__ void tile_gather_kernel(const double* __restrict__ pts, const int32_t* __restrict__ perm,
+                                   int64_t n, int64_t t0, TileBatch tb) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)tb.C * tb.TP) return;
+  const int64_t t = gid / tb.TP;
+  const int j = (int)(gid % tb.TP);
+  const int64_t g = (t0 + t) * tb.TP + j;
+  const bool v = g < n;
+  const int64_t p = perm[v ? g : (t0 + t) * tb.TP];
+  tb.xyz[3 * gid] = pts[3 * p];
+  tb.xyz[3 * gid + 1] = pts[3 * p + 1];
+  tb.xyz[3 * gid + 2] = pts[3 * p + 2];
+  tb.out[gid] = v ? p : -1;
+}
+
+// Cubic grid: tile = TX x TY x TZ block of grid points (z fastest).
+__global__ void tile_cubic_kernel(PointSrc src, int nx, int TX, int TY, int TZ, int nby, int nbz,
+                                  int64_t t0, TileBatch tb) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)tb.C * tb.TP) return;
+  const int64_t t = t0 + gid / tb.TP;
+  const int j = (int)(gid % tb.TP);
+  const int64_t bz = t % nbz, by = (t / nbz) % nby, bx = t / ((int64_t)nbz * nby);
+  const int iz = j % TZ, iy = (j / TZ) % TY, ix = j / (TZ * TY);
+  int64_t i = bx * TX + ix, k = by * TY + iy, l = bz * TZ + iz;
+  const bool v = i < nx && k < src.ny && l < src.nz;
+  if (!v) { i = bx * TX; k = by * TY; l = bz * TZ; }
+  const double fi = (double)i, fj = (double)k, fk = (double)l;
+  tb.xyz[3 * gid] = src.o[0] + fi * src.ax[0] + fj * src.ax[3] + fk * src.ax[6];
+  tb.xyz[3 * gid + 1] = src.o[1] + fi * src.ax[1] + fj * src.ax[4] + fk * src.ax[7];
+  tb.xyz[3 * gid + 2] = src.o[2] + fi * src.ax[2] + fj * src.ax[5] + fk * src.ax[8];
+  tb.out[gid] = v ? (i * src.ny + k) * (int64_t)src.nz + l : -1;
+}
+
+// One CTA per tile: bounding sphere of the tile's points, then the ordered
+// list of segments whose screening sphere meets it.
+__global__ void __launch_bounds__(kTileThreads)
+    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb, int rows,
+                  double* __restrict__ stats) {
+  using Scan = cub::BlockScan<int, kTileThreads>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ double red[3][kTileThreads / 32];
+  __shared__ double sctr[3], srad;
+  __shared__ int base_s, base_k;
+  const int t = blockIdx.x, TP = tb.TP;
+  const double* xyz = tb.xyz + (int64_t)t * TP * 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // centre = mean of the tile's points (padding repeats a real point)
+  double c[3] = {0, 0, 0};
+  for (int j = threadIdx.x; j < TP; j += kTileThreads)
+    for (int d = 0; d < 3; ++d) c[d] += xyz[3 * j + d];
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) c[d] += __shfl_xor_sync(0xffffffffu, c[d], o);
+    if (lane == 0) red[d][warp] = c[d];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double acc = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) acc += red[threadIdx.x][w];
+    sctr[threadIdx.x] = acc / TP;
+  }
+  __syncthreads();
+  double r2 = 0.0;
+  for (int j = threadIdx.x; j < TP; j += kTileThreads) {
+    const double dx = xyz[3 * j] - sctr[0], dy = xyz[3 * j + 1] - sctr[1], dz = xyz[3 * j + 2] - sctr[2];
+    r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+  }
+  for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+  if (lane == 0) red[0][warp] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) m = fmax(m, red[0][w]);
+    srad = sqrt(m) * (1.0 + 1e-12) + 1e-9;
+    base_s = 0;
+    base_k = 0;
+  }
+  __syncthreads();
+  const double rad = srad;
+  int32_t* sl = tb.segs + (int64_t)t * nseg;
+  int32_t* k0 = tb.k0 + (int64_t)t * nseg;
+  int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+  for (int s0 = 0; s0 < nseg; s0 += kTileThreads) {
+    const int s = s0 + threadIdx.x;
+    int sig = 0, nc = 0;
+    DevSeg sg;
+    if (s < nseg) {
+      sg = segs[s];
+      const double dx = sg.cx - sctr[0], dy = sg.cy - sctr[1], dz = sg.cz - sctr[2];
+      const double d = sqrt(dx * dx + dy * dy + dz * dz);
+      const double lim = sqrt(sg.rcut2) + rad;
+      if (d <= lim) {
+        sig = 1;
+        nc = ncomp_of_type_dev(sg.type);
+      }
+    }
+    // pack (segment count, AO count) into one int: both sums stay below 2^16
+    int packed, ptot;
+    Scan(scan_tmp).ExclusiveSum((sig << 16) | nc, packed, ptot);
+    const int2 pos = make_int2(packed >> 16, packed & 0xffff);
+    const int2 tot = make_int2(ptot >> 16, ptot & 0xffff);
+    if (sig) {
+      const int ks = base_k + pos.y;
+      sl[base_s + pos.x] = s;
+      k0[base_s + pos.x] = ks;
+      for (int q = 0; q < nc; ++q) am[ks + q] = sg.ao0 + q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      base_s += tot.x;
+      base_k += tot.y;
+    }
+    __syncthreads();
+  }
+  const int kt_true = base_k;
+  const int kt = (kt_true + kKtAlign - 1) / kKtAlign * kKtAlign;
+  for (int k = kt_true + threadIdx.x; k < kt; k += kTileThreads) am[k] = -1;
+  if (threadIdx.x == 0) {
+    tb.nsig[t] = base_s;
+    tb.ktrue[t] = kt_true;
+    tb.kt[t] = kt;
+    int npts = 0;
+    for (int j = 0; j < TP; ++j) npts += tb.out[(int64_t)t * TP + j] >= 0;
+    atomicAdd(&stats[0], 1.0);
+    atomicAdd(&stats[1], (double)npts);
+    atomicAdd(&stats[2], (double)kt_true);
+    atomicAdd(&stats[3], (double)rows * (double)kt * (double)kt);
+  }
+}
+
+// ------------------------------------------------------------------ FP64 contraction kernel
+constexpr int BM = 128, BN = 64, BK = 32, STAGES = 3;
+constexpr int A_LD = BK + 4;  // 36 doubles: conflict-free fragment loads
+constexpr int B_LD = BN + 4;  // 68 doubles
+constexpr int C_LD = BN + 1;
+constexpr int A_STAGE = BM * A_LD, B_STAGE = BK * B_LD;
+constexpr int kThreads = 256;
+constexpr size_t kSmemPipe = sizeof(double) * STAGES * (A_STAGE + B_STAGE);
+constexpr size_t kSmemC = sizeof(double) * BM * C_LD;
+constexpr size_t kSmemFp64 = kSmemPipe > kSmemC ? kSmemPipe : kSmemC;
+static_assert(kKtAlign % BN == 0 && kKtAlign % BK == 0, "tile K alignment");
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int sz = valid ? 8 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// One CTA per tile of PTS = 128/NQA points; tile row r holds quantity r / PTS
+// of point r % PTS (quantity 0 = phi, 1..3 = d_k phi).  It sweeps the tile's
+// compact nu range in 64-column slices, each with a full K loop over the
+// compact mu range (B = D gathered by index), and reduces every finished G
+// slice against the AO values of its columns.
+// Inputs of the force epilogue (EPI = 1): per-point dL/drho and dL/dgrad rho
+// indexed by the original point index, AO -> atom map, dL/dR accumulator.
+struct ForceArgs {
+  const double* v_rho = nullptr;
+  const double* v_grad = nullptr;
+  const int32_t* ao_atom = nullptr;
+  double* dLdR = nullptr;
+  int natom = 0;
+};
+constexpr int kMaxSmemAtoms = 1024;
+
+template <int NQA, int EPI>
+__global__ void __launch_bounds__(kThreads)
+    fp64_tile_kernel(TileBatch tb, const double* __restrict__ D, int Mpad, ctc_outputs out,
+                     ctc_params prm, ForceArgs fa) {
+  constexpr int PTS = BM / NQA;
+  constexpr int TPP = kThreads / PTS;  // epilogue threads per point
+  constexpr int NS = NQA == 4 ? 16 : 4;
+  extern __shared__ __align__(16) double smem[];
+  double* sA = smem;
+  double* sB = smem + STAGES * A_STAGE;
+  double* sC = smem;  // aliases the pipeline after the K loop
+  __shared__ int s_colmap[BN];
+  __shared__ double s_force[EPI == 1 ? 3 * kMaxSmemAtoms : 1];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 3, wn = warp >> 2;
+  const int t = blockIdx.x;
+  const int kt = tb.kt[t];
+  const int nq_ao = tb.nq;
+  const int64_t ldq = (int64_t)PTS * tb.Kcap;  // stride between quantities
+  const double* A = tb.ao + (int64_t)t * nq_ao * ldq;
+  const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+
+  const int epl = tid / TPP, esub = tid % TPP;
+  double acc_s[NS];
+#pragma unroll
+  for (int i = 0; i < NS; ++i) acc_s[i] = 0.0;
+  // force epilogue: per-point weights, per-CTA atom accumulators
+  const bool force_smem = EPI == 1 && fa.natom <= kMaxSmemAtoms;
+  double fvr = 0.0, fvg[3] = {0.0, 0.0, 0.0};
+  if constexpr (EPI == 1) {
+    for (int i = tid; i < 3 * fa.natom && force_smem; i += kThreads) s_force[i] = 0.0;
+    const int64_t oi = tb.out[(int64_t)t * PTS + epl];
+    if (oi >= 0) {
+      fvr = fa.v_rho[oi];
+      if (fa.v_grad)
+        for (int k = 0; k < 3; ++k) fvg[k] = fa.v_grad[3 * oi + k];
+    }
+  }
+
+  const int nkb = kt / BK;
+  for (int n0 = 0; n0 < kt; n0 += BN) {
+    if (tid < BN) s_colmap[tid] = am[n0 + tid];
+    __syncthreads();
+    double c[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) c[i][j][0] = c[i][j][1] = 0.0;
+
+    auto load_stage = [&](int stage, int kb) {
+      double* a = sA + stage * A_STAGE;
+      double* b = sB + stage * B_STAGE;
+      const int k0 = kb * BK;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int ch = tid + i * kThreads;
+        const int r = ch >> 4, cc = (ch & 15) * 2;
+        const int q = r / PTS, pl = r % PTS;
+        cp_async16(a + r * A_LD + cc, A + q * ldq + (int64_t)pl * tb.Kcap + k0 + cc, true);
+      }
+      // B gather: 32 rows (compact mu) x 64 columns (compact nu), 8 bytes each
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int e = tid + i * kThreads;
+        const int r = e >> 6, cc = e & 63;
+        const int mu = am[k0 + r], nu = s_colmap[cc];
+        const bool v = mu >= 0 && nu >= 0;
+        cp_async8(b + r * B_LD + cc, D + (v ? (int64_t)mu * Mpad + nu : 0), v);
+      }
+    };
+
+    load_stage(0, 0);
+    cp_async_commit();
+    if (nkb > 1) load_stage(1, 1);
+    cp_async_commit();
+    for (int kb = 0; kb < nkb; ++kb) {
+      if (kb + 2 < nkb) load_stage((kb + 2) % STAGES, kb + 2);
+      cp_async_commit();
+      cp_async_wait<2>();
+      __syncthreads();
+      const double* a = sA + (kb % STAGES) * A_STAGE;
+      const double* b = sB + (kb % STAGES) * B_STAGE;
+#pragma unroll
+      for (int ks = 0; ks < BK; ks += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          af[i] = a[(wm * 32 + i * 8 + (lane >> 2)) * A_LD + ks + (lane & 3)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          bf[j] = b[(ks + (lane & 3)) * B_LD + wn * 32 + j * 8 + (lane >> 2)];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(c[i][j][0], c[i][j][1], af[i], bf[j]);
+      }
+      __syncthreads();
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int r = wm * 32 + i * 8 + (lane >> 2);
+        const int cc = wn * 32 + j * 8 + 2 * (lane & 3);
+        sC[r * C_LD + cc] = c[i][j][0];
+        sC[r * C_LD + cc + 1] = c[i][j][1];
+      }
+    __syncthreads();
+    if constexpr (EPI == 0) {
+      {
+        const double* aop = A + (int64_t)epl * tb.Kcap + n0;
+        for (int v = esub; v < BN; v += TPP) {
+          const double G0 = sC[(0 * PTS + epl) * C_LD + v];
+          const double phi = aop[v];
+          acc_s[0] += G0 * phi;
+          if (nq_ao >= 4) {
+            const double d0 = aop[ldq + v], d1 = aop[2 * ldq + v], d2 = aop[3 * ldq + v];
+            acc_s[1] += G0 * d0;
+            acc_s[2] += G0 * d1;
+            acc_s[3] += G0 * d2;
+            if constexpr (NQA == 4) {
+              const double G1 = sC[(1 * PTS + epl) * C_LD + v];
+              const double G2 = sC[(2 * PTS + epl) * C_LD + v];
+              const double G3 = sC[(3 * PTS + epl) * C_LD + v];
+              acc_s[10] += G1 * d0;
+              acc_s[11] += G1 * d1;
+              acc_s[12] += G1 * d2;
+              acc_s[13] += G2 * d1;
+              acc_s[14] += G2 * d2;
+              acc_s[15] += G3 * d2;
+              if (nq_ao == 10) {
+  #pragma unroll
+                for (int h = 0; h < 6; ++h) acc_s[4 + h] += G0 * aop[(4 + h) * ldq + v];
+              }
+            }
+          }
+        }
+      }
+    } else {
+      // dL/dR_A,j += sum over nu on atom A of
+      //   -2 v_rho d_j phi G0 - 2 sum_k v_k (d_j d_k phi G0 + d_j phi G_k)
+      const double* aop = A + (int64_t)epl * tb.Kcap + n0;
+      const int hidx[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
+      for (int v = esub; v < BN; v += TPP) {
+        const int nu = s_colmap[v];
+        if (nu < 0 || (fvr == 0.0 && fvg[0] == 0.0 && fvg[1] == 0.0 && fvg[2] == 0.0)) continue;
+        const int atom = fa.ao_atom[nu];
+        if (atom < 0) continue;
+        const double G0 = sC[(0 * PTS + epl) * C_LD + v];
+        double Gk[3] = {0.0, 0.0, 0.0};
+        if constexpr (NQA == 4) {
+          Gk[0] = sC[(1 * PTS + epl) * C_LD + v];
+          Gk[1] = sC[(2 * PTS + epl) * C_LD + v];
+          Gk[2] = sC[(3 * PTS + epl) * C_LD + v];
+        }
+        for (int j = 0; j < 3; ++j) {
+          const double dj = aop[(1 + j) * ldq + v];
+          double c = -2.0 * fvr * dj * G0;
+          if (fa.v_grad) {
+            for (int k = 0; k < 3; ++k)
+              c -= 2.0 * fvg[k] * (aop[hidx[j][k] * ldq + v] * G0 + dj * Gk[k]);
+          }
+          if (force_smem) atomicAdd(&s_force[3 * atom + j], c);
+          else atomicAdd(&fa.dLdR[3 * atom + j], c);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if constexpr (EPI == 1) {
+    __syncthreads();
+    if (force_smem)
+      for (int i = tid; i < 3 * fa.natom; i += kThreads)
+        if (s_force[i] != 0.0) atomicAdd(&fa.dLdR[i], s_force[i]);
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < NS; ++i)
+#pragma unroll
+    for (int off = TPP / 2; off > 0; off >>= 1)
+      acc_s[i] += __shfl_xor_sync(0xffffffffu, acc_s[i], off);
+  const int64_t oidx = tb.out[(int64_t)t * PTS + epl];
+  if (esub == 0 && oidx >= 0) {
+    double s[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) s[i] = i < NS ? acc_s[i] : 0.0;
+    finalize_point(s, NQA, nq_ao, out, oidx, prm);
+  }
+}
+
+// ------------------------------------------------------------------ chunk scratch
+
+struct Carve {
+  char* p;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) / 256 * 256;
+    T* r = (T*)(p + off);
+    off += sizeof(T) * count;
+    return r;
+  }
+};
+
+size_t tile_bytes(const ctc_molecule* mol, int C, int TP) {
+  const size_t Kcap = mol->Mpad;
+  size_t b = 0;
+  auto add = [&](size_t x) { b = (b + 255) / 256 * 256 + x; };
+  add(sizeof(double) * C * TP * 3);
+  add(sizeof(int64_t) * C * TP);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * C);
+  add(sizeof(int32_t) * (size_t)C * mol->nseg);
+  add(sizeof(int32_t) * (size_t)C * mol->nseg);
+  add(sizeof(int32_t) * (size_t)C * Kcap);
+  return b + 256;
+}
+
+
+// Tile builder + chunk loop.  For every chunk: tile points, screen, AO block
+// (derivative order deriv, nq quantities), then compute(tb).
+inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, int nq, int deriv,
+                     cudaStream_t st, const std::function<int(const TileBatch&)>& compute) {
+  int TX = 2, TY = 4, TZ = 4;
+  if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
+  int64_t ntiles, nbx = 0, nby = 0, nbz = 0;
+  int nx = 0;
+  if (src.cubic) {
+    nx = (int)(n / ((int64_t)src.ny * src.nz));
+    nbx = (nx + TX - 1) / TX;
+    nby = (src.ny + TY - 1) / TY;
+    nbz = (src.nz + TZ - 1) / TZ;
+    ntiles = nbx * nby * nbz;
+  } else {
+    ntiles = (n + TP - 1) / TP;
+  }
+  // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within ~6 GB
+  // (CTC_CHUNK_BYTES overrides), at least one full wave of CTAs on 148 SMs
+  const size_t ao_per_tile = sizeof(double) * (size_t)nq * TP * mol->Mpad;
+  size_t budget = (size_t)6 << 30;
+  if (const char* env = std::getenv("CTC_CHUNK_BYTES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) budget = (size_t)v;
+  }
+  int64_t C = std::max<int64_t>(148, (int64_t)(budget / ao_per_tile));
+  C = std::min<int64_t>(C, ntiles);
+  int rc;
+  if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;
+  if ((rc = mol->ws_misc.ensure(tile_bytes(mol, (int)C, TP), st)) != CTC_OK) return rc;
+  TileBatch tb;
+  tb.TP = TP;
+  tb.Kcap = mol->Mpad;
+  tb.nq = nq;
+  tb.ao = (double*)mol->ws_ao.p;
+  {
+    Carve cv{(char*)mol->ws_misc.p};
+    tb.xyz = cv.take<double>((size_t)C * TP * 3);
+    tb.out = cv.take<int64_t>((size_t)C * TP);
+    tb.nsig = cv.take<int32_t>(C);
+    tb.ktrue = cv.take<int32_t>(C);
+    tb.kt = cv.take<int32_t>(C);
+    tb.segs = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.k0 = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.aomap = cv.take<int32_t>((size_t)C * tb.Kcap);
+  }
+  // explicit points: Morton order over the molecule's box padded by 12 bohr
+  int32_t* perm = nullptr;
+  if (!src.cubic) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int a = 0; a < mol->natom; ++a)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], mol->atom_xyz[3 * a + d]);
+        hi[d] = std::max(hi[d], mol->atom_xyz[3 * a + d]);
+      }
+    if (mol->natom == 0)
+      for (int d = 0; d < 3; ++d) { lo[d] = -1; hi[d] = 1; }
+    double ext = 0;
+    for (int d = 0; d < 3; ++d) {
+      lo[d] -= 12.0;
+      hi[d] += 12.0;
+      ext = std::max(ext, hi[d] - lo[d]);
+    }
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 30, st);
+    const size_t need = 4 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
+    if ((rc = mol->ws_part.ensure(need, st)) != CTC_OK) return rc;
+    Carve cv{(char*)mol->ws_part.p};
+    uint32_t* k_in = cv.take<uint32_t>(n);
+    uint32_t* k_out = cv.take<uint32_t>(n);
+    int32_t* v_in = cv.take<int32_t>(n);
+    perm = cv.take<int32_t>(n);
+    void* tmp = cv.take<char>(tmp_bytes);
+    morton_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src.pts, n, lo[0], lo[1], lo[2],
+                                                                1024.0 / ext, k_in, v_in);
+    CTC_CUDA_TRY(cudaGetLastError());
+    CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
+                                                 30, st));
+    mol->host_launches += 2;
+  }
+  for (int64_t t0 = 0; t0 < ntiles; t0 += C) {
+    tb.C = (int)std::min<int64_t>(C, ntiles - t0);
+    const int64_t npts = (int64_t)tb.C * TP;
+    const unsigned g = (unsigned)((npts + 255) / 256);
+    if (src.cubic)
+      tile_cubic_kernel<<<g, 256, 0, st>>>(src, nx, TX, TY, TZ, (int)nby, (int)nbz, t0, tb);
+    else
+      tile_gather_kernel<<<g, 256, 0, st>>>(src.pts, perm, n, t0, tb);
+    CTC_CUDA_TRY(cudaGetLastError());
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, 128, mol->d_stats);
+    CTC_CUDA_TRY(cudaGetLastError());
+    {
+      ProfScope ps(mol, 1, st);
+      if ((rc = launch_ao_tiles(mol, tb, deriv, st)) != CTC_OK) return rc;
+    }
+    mol->host_launches += 3;
+    mol->host_chunks += 1;
+    if ((rc = compute(tb)) != CTC_OK) return rc;
+  }
+  return CTC_OK;
+}
+
+}  // namespace
+}  // namespace ctc
