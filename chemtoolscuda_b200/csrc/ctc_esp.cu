@@ -24,6 +24,8 @@
 // V(C) = sum_A Z_A / |C - R_A| - electronic part (src/evaluate_electrostatic.cu:10357-10369).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -267,9 +269,14 @@ void seg_monomials(int type, std::vector<Mono>& monos, std::vector<double>& Tm /
 
 struct PairOut {
   int L;
+  double bound;  // upper bound of |pair contribution| at any point
   EspPair pr;
   std::vector<double> h;
 };
+
+// Upper bound of |R^0_tuv(p, X)| over all points for t + u + v = s, used to
+// bound a pair's contribution: (2p)^(s/2) times a generous constant in s.
+inline double r_bound(double p, int s) { return std::pow(2.0 * p + 1.0, 0.5 * s) * std::pow(3.0, s); }
 
 }  // namespace
 
@@ -294,7 +301,8 @@ static int build_esp(ctc_molecule* mol) {
   std::vector<std::vector<Mono>> monos(nseg);
   std::vector<std::vector<double>> Tm(nseg);
   for (int s = 0; s < nseg; ++s) seg_monomials(mol->segs[s].type, monos[s], Tm[s]);
-  const double eps = 1e-17;
+  const double eps = 1e-22;            // pre-filter before the Hermite densities are formed
+  const double budget = 1e-11;         // total |ESP| error allowed for the pairs dropped below
   unsigned nthr = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
   std::vector<std::vector<PairOut>> outs(nthr);
   auto worker = [&](unsigned tid) {
@@ -360,6 +368,13 @@ static int build_esp(ctc_molecule* mol) {
                 }
               }
             }
+            double bnd = 0.0;
+            for (int tt = 0; tt <= L; ++tt)
+              for (int uu = 0; uu <= L - tt; ++uu)
+                for (int vv = 0; vv <= L - tt - uu; ++vv)
+                  bnd += std::fabs(po.h[tuv_index(tt, uu, vv)]) * r_bound(p, tt + uu + vv);
+            po.bound = bnd * pref;
+            if (po.bound < eps) continue;
             outs[tid].push_back(std::move(po));
           }
         }
@@ -369,6 +384,22 @@ static int build_esp(ctc_molecule* mol) {
   std::vector<std::thread> th;
   for (unsigned t = 0; t < nthr; ++t) th.emplace_back(worker, t);
   for (auto& t : th) t.join();
+  // drop the weakest pairs while their summed bound stays within the budget
+  {
+    std::vector<double> bounds;
+    for (auto& o : outs)
+      for (auto& po : o) bounds.push_back(po.bound);
+    std::sort(bounds.begin(), bounds.end());
+    double acc = 0.0, cut = 0.0;
+    for (double b : bounds) {
+      if (acc + b > budget) break;
+      acc += b;
+      cut = b;
+    }
+    for (auto& o : outs)
+      o.erase(std::remove_if(o.begin(), o.end(), [&](const PairOut& po) { return po.bound <= cut; }),
+              o.end());
+  }
   // gather, sorted by L, into batches of equal L
   std::vector<EspPair> pairs;
   std::vector<double> hv;
@@ -421,6 +452,9 @@ static int build_esp(ctc_molecule* mol) {
     return rc;
   }
   mol->esp_valid = true;
+  if (std::getenv("CTC_LOG"))
+    std::fprintf(stderr, "[ctc] esp tables: %d primitive pairs, %d batches, %zu Hermite coefficients\n",
+                 e->npairs, e->nbatch, e->nh);
   return CTC_OK;
 }
 
