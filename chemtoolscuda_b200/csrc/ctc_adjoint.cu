@@ -30,14 +30,14 @@ __global__ void densify_kernel(TileBatch tb, const double* __restrict__ v_rho,
   const double* A = tb.ao + (int64_t)t * tb.nq * ldq;
   const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
   for (int idx = threadIdx.x; idx < TP * kt; idx += blockDim.x) {
-    const int j = idx / kt, k = idx % kt;
+    const int j = idx % TP, k = idx / TP;
     const int mu = am[k];
     const int64_t oi = tb.out[(int64_t)t * TP + j];
     if (mu < 0 || oi < 0) continue;
-    const double phi = A[(int64_t)j * tb.Kcap + k];
+    const double phi = A[(int64_t)k * TP + j];
     double w = v_rho[oi] * phi;
     if (v_grad)
-      for (int d = 0; d < 3; ++d) w += 2.0 * v_grad[3 * oi + d] * A[(1 + d) * ldq + (int64_t)j * tb.Kcap + k];
+      for (int d = 0; d < 3; ++d) w += 2.0 * v_grad[3 * oi + d] * A[(1 + d) * ldq + (int64_t)k * TP + j];
     const int64_t row = ((int64_t)t * TP + j) * Mpad;
     Phi[row + mu] = phi;
     W[row + mu] = w;
@@ -122,11 +122,12 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// dLdD in the caller's AO order from the accumulator in internal order.
 __global__ void symmetrize_add_kernel(const double* __restrict__ Cacc, int M, int Mpad,
-                                      double* __restrict__ dLdD) {
+                                      const int32_t* __restrict__ iperm, double* __restrict__ dLdD) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (int64_t)M * M) return;
-  const int r = (int)(i / M), c = (int)(i % M);
+  const int r = iperm[i / M], c = iperm[i % M];
   dLdD[i] += 0.5 * (Cacc[(int64_t)r * Mpad + c] + Cacc[(int64_t)c * Mpad + r]);
 }
 
@@ -223,7 +224,8 @@ int eval_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const dou
   if (rc != CTC_OK) return rc;
   if (dLdD) {
     const int64_t MM = (int64_t)mol->M * mol->M;
-    symmetrize_add_kernel<<<(unsigned)((MM + 255) / 256), 256, 0, st>>>(Cacc, mol->M, Mpad, dLdD);
+    symmetrize_add_kernel<<<(unsigned)((MM + 255) / 256), 256, 0, st>>>(Cacc, mol->M, Mpad,
+                                                                         mol->d_ao_iperm, dLdD);
     CTC_CUDA_TRY(cudaGetLastError());
   }
   return CTC_OK;

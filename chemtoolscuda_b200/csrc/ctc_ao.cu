@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(kAoThreads)
   for (int64_t p = p_begin; p < p_end; ++p) {
     double px, py, pz;
     point_of(src, p, px, py, pz);
-    eval_segment<DERIV>(sg, alpha, coef, px, py, pz, out + p * ld_point + sg.ao0, ld_q, nq_out);
+    eval_segment<DERIV>(sg, alpha, coef, px, py, pz, out + p * ld_point + sg.orig_ao0, ld_q, nq_out);
   }
 }
 
@@ -137,7 +137,7 @@ template <int DERIV, int TYPE>
 __device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __restrict__ alpha,
                                            const double* __restrict__ coef, double px, double py,
                                            double pz, double* __restrict__ o, int64_t ld_q,
-                                           int nq_out) {
+                                           int64_t ldc, int nq_out) {
   constexpr int L = TYPE == 0 ? 0 : (TYPE == 1 ? 1 : (TYPE <= 3 ? 2 : (TYPE <= 5 ? 3 : 4)));
   constexpr int NC = TYPE == 0 ? 1 : TYPE == 1 ? 3 : TYPE == 2 ? 6 : TYPE == 3 ? 5
                      : TYPE == 4 ? 10 : TYPE == 5 ? 7 : TYPE == 6 ? 15 : 9;
@@ -147,7 +147,7 @@ __device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __res
   if (r2 > sg.rcut2) {
     for (int q = 0; q < nq_out; ++q)
 #pragma unroll
-      for (int j = 0; j < NC; ++j) o[q * ld_q + j] = 0.0;
+      for (int j = 0; j < NC; ++j) o[q * ld_q + j * ldc] = 0.0;
     return;
   }
   double R0 = 0.0, R1 = 0.0, R2 = 0.0;
@@ -167,38 +167,40 @@ __device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __res
     Y[i] = Y[i - 1] * y;
     Z[i] = Z[i - 1] * z;
   }
-  if constexpr (TYPE == 0) ao_poly_0<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 1) ao_poly_1<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 2) ao_poly_2<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 3) ao_poly_3<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 4) ao_poly_4<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 5) ao_poly_5<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else if constexpr (TYPE == 6) ao_poly_6<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
-  else ao_poly_7<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, nq_out);
+  if constexpr (TYPE == 0) ao_poly_0<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 1) ao_poly_1<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 2) ao_poly_2<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 3) ao_poly_3<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 4) ao_poly_4<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 5) ao_poly_5<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else if constexpr (TYPE == 6) ao_poly_6<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  else ao_poly_7<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
 }
 
 template <int DERIV>
 __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __restrict__ alpha,
                                               const double* __restrict__ coef, double px, double py,
                                               double pz, double* __restrict__ o, int64_t ld_q,
-                                              int nq_out) {
+                                              int64_t ldc, int nq_out) {
   switch (sg.type) {
-    case 0: eval_typed<DERIV, 0>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 1: eval_typed<DERIV, 1>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 2: eval_typed<DERIV, 2>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 3: eval_typed<DERIV, 3>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 4: eval_typed<DERIV, 4>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 5: eval_typed<DERIV, 5>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    case 6: eval_typed<DERIV, 6>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
-    default: eval_typed<DERIV, 7>(sg, alpha, coef, px, py, pz, o, ld_q, nq_out); break;
+    case 0: eval_typed<DERIV, 0>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 1: eval_typed<DERIV, 1>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 2: eval_typed<DERIV, 2>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 3: eval_typed<DERIV, 3>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 4: eval_typed<DERIV, 4>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 5: eval_typed<DERIV, 5>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 6: eval_typed<DERIV, 6>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    default: eval_typed<DERIV, 7>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
   }
 }
 
 // One CTA per tile; each warp takes one significant segment at a time and
-// its lanes take the tile's points, so a warp always runs one segment type.
-// Padding columns [ktrue, kt) are zeroed.
+// its lanes take the tile's points, so a warp always runs one segment type
+// and its stores of one (quantity, AO) cover consecutive points.  Layout of
+// the tile block: A[q][k][point] (point fastest).  Padding columns
+// [ktrue, kt) are zeroed.
 template <int DERIV>
-__global__ void __launch_bounds__(kAoThreads)
+__global__ void __launch_bounds__(kAoThreads, 3)
     ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
                    const double* __restrict__ coef, TileBatch tb) {
   const int t = blockIdx.x;
@@ -212,17 +214,16 @@ __global__ void __launch_bounds__(kAoThreads)
   for (int pg = 0; pg < TP; pg += 32) {
     const int j = pg + lane;
     const double px = xyz[3 * j], py = xyz[3 * j + 1], pz = xyz[3 * j + 2];
-    double* row = A + (int64_t)j * tb.Kcap;
     for (int i = warp; i < ns; i += kAoThreads / 32) {
       const DevSeg sg = segs[sl[i]];
-      eval_dispatch<DERIV>(sg, alpha, coef, px, py, pz, row + k0[i], ld_q, tb.nq);
+      eval_dispatch<DERIV>(sg, alpha, coef, px, py, pz, A + (int64_t)k0[i] * TP + j, ld_q, TP, tb.nq);
     }
   }
   const int kt_true = tb.ktrue[t], kt = tb.kt[t];
-  const int npad = kt - kt_true;
-  for (int idx = threadIdx.x; idx < tb.nq * TP * npad; idx += kAoThreads) {
-    const int c = idx % npad, r = idx / npad;  // r = q * TP + j
-    A[(int64_t)r * tb.Kcap + kt_true + c] = 0.0;
+  const int npad = (kt - kt_true) * TP;
+  for (int idx = threadIdx.x; idx < tb.nq * npad; idx += kAoThreads) {
+    const int q = idx / npad, r = idx % npad;
+    A[q * ld_q + (int64_t)kt_true * TP + r] = 0.0;
   }
 }
 

@@ -190,6 +190,8 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
       sg.nprim = K;
       sg.prim0 = (int)m->alpha.size();
       sg.ao0 = ao;
+      sg.orig_ao0 = ao;
+      sg.pad = 0;
       sg.atom = atom;
       std::vector<double> aa, cc;
       for (int k = 0; k < K; ++k) {
@@ -206,7 +208,6 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
       m->alpha.insert(m->alpha.end(), aa.begin(), aa.end());
       m->coef.insert(m->coef.end(), cc.begin(), cc.end());
       m->segs.push_back(sg);
-      for (int j = 0; j < ncomp_of_type(t); ++j) m->ao_atom.push_back(atom);
       ao += ncomp_of_type(t);
     }
     ia += S;
@@ -221,19 +222,82 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
   m->M = ao;
   m->Mpad = (ao + 127) / 128 * 128;
   m->nseg = (int)m->segs.size();
+  // Internal AO order: segments grouped by atom, atoms in Morton order of
+  // their positions, so that the AOs significant on a compact point tile form
+  // few contiguous runs (gathers of D rows/columns then touch whole sectors).
+  {
+    std::vector<uint64_t> key(natom, 0);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int a = 0; a < natom; ++a)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], atom_xyz[3 * a + d]);
+        hi[d] = std::max(hi[d], atom_xyz[3 * a + d]);
+      }
+    auto spread = [](uint64_t v) {
+      uint64_t r = 0;
+      for (int b = 0; b < 21; ++b) r |= ((v >> b) & 1ull) << (3 * b);
+      return r;
+    };
+    for (int a = 0; a < natom; ++a) {
+      uint64_t q[3];
+      for (int d = 0; d < 3; ++d) {
+        const double ext = std::max(hi[d] - lo[d], 1e-9);
+        q[d] = (uint64_t)std::min(2097151.0, std::max(0.0, (atom_xyz[3 * a + d] - lo[d]) / ext * 2097151.0));
+      }
+      key[a] = spread(q[0]) | (spread(q[1]) << 1) | (spread(q[2]) << 2);
+    }
+    std::vector<int> rank_of(natom);
+    {
+      std::vector<int> order(natom);
+      for (int a = 0; a < natom; ++a) order[a] = a;
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+      for (int r = 0; r < natom; ++r) rank_of[order[r]] = r;
+    }
+    std::vector<int> so(m->nseg);
+    for (int i = 0; i < m->nseg; ++i) so[i] = i;
+    std::stable_sort(so.begin(), so.end(), [&](int x, int y) {
+      const int ax = m->segs[x].atom, ay = m->segs[y].atom;
+      const int rx = ax < 0 ? natom : rank_of[ax], ry = ay < 0 ? natom : rank_of[ay];
+      return rx < ry;
+    });
+    std::vector<DevSeg> ns;
+    m->ao_perm.assign(ao, 0);
+    std::vector<int32_t> new_atom;
+    int k = 0;
+    for (int i : so) {
+      DevSeg sg = m->segs[i];
+      sg.orig_ao0 = sg.ao0;
+      sg.ao0 = k;
+      const int nc = ncomp_of_type(sg.type);
+      for (int j = 0; j < nc; ++j) {
+        m->ao_perm[k + j] = sg.orig_ao0 + j;
+        new_atom.push_back(sg.atom);
+      }
+      k += nc;
+      ns.push_back(sg);
+    }
+    m->segs.swap(ns);
+    m->ao_atom.swap(new_atom);
+  }
   m->seg_order.resize(m->nseg);
   for (int i = 0; i < m->nseg; ++i) m->seg_order[i] = i;
   std::stable_sort(m->seg_order.begin(), m->seg_order.end(), [&](int x, int y) {
     if (m->segs[x].type != m->segs[y].type) return m->segs[x].type < m->segs[y].type;
     return m->segs[x].nprim < m->segs[y].nprim;
   });
-  m->D.assign(D, D + (size_t)ao * ao);
+  m->D.resize((size_t)ao * ao);
+  for (int i = 0; i < ao; ++i) {
+    const double* src = D + (size_t)m->ao_perm[i] * ao;
+    for (int j = 0; j < ao; ++j) m->D[(size_t)i * ao + j] = src[m->ao_perm[j]];
+  }
   m->ao_atom.resize(m->Mpad, -1);
+  std::vector<int32_t> iperm(ao);
+  for (int i = 0; i < ao; ++i) iperm[m->ao_perm[i]] = i;
 
   size_t MM = (size_t)m->Mpad * m->Mpad;
   std::vector<double> Dpad(MM, 0.0);
   for (int i = 0; i < ao; ++i)
-    std::memcpy(&Dpad[(size_t)i * m->Mpad], D + (size_t)i * ao, sizeof(double) * ao);
+    std::memcpy(&Dpad[(size_t)i * m->Mpad], &m->D[(size_t)i * ao], sizeof(double) * ao);
 #define ALLOC_COPY(dst, src, count)                                                          \
   do {                                                                                       \
     cudaError_t _e = cudaMalloc((void**)&(dst), sizeof(*(dst)) * (count));                   \
@@ -250,6 +314,7 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
   ALLOC_COPY(m->d_order, m->seg_order.data(), m->seg_order.size());
   ALLOC_COPY(m->d_ao_atom, m->ao_atom.data(), m->ao_atom.size());
   ALLOC_COPY(m->d_D, Dpad.data(), MM);
+  ALLOC_COPY(m->d_ao_iperm, iperm.data(), iperm.size());
 #undef ALLOC_COPY
   if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
       cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess ||
@@ -273,6 +338,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   cudaFree(m->d_order);
   cudaFree(m->d_ao_atom);
   cudaFree(m->d_D);
+  cudaFree(m->d_ao_iperm);
   cudaFree(m->d_Dsl);
   cudaFree(m->d_Dscale);
   cudaFree(m->d_status);
@@ -291,10 +357,20 @@ int ctc_molecule_natom(const ctc_molecule* m) { return m ? m->natom : fail(CTC_E
 int ctc_molecule_set_density_matrix(ctc_molecule* m, const double* d_D, void* stream) {
   if (!m || !d_D) return fail(CTC_ERR_INVALID, "set_density_matrix: null argument");
   cudaStream_t st = (cudaStream_t)stream;
-  CTC_CUDA_TRY(cudaMemcpy2DAsync(m->d_D, sizeof(double) * m->Mpad, d_D, sizeof(double) * m->M,
-                                 sizeof(double) * m->M, m->M, cudaMemcpyDeviceToDevice, st));
-  CTC_CUDA_TRY(cudaMemcpyAsync(m->D.data(), d_D, sizeof(double) * m->M * m->M,
-                               cudaMemcpyDeviceToHost, st));
+  const int M = m->M, Mp = m->Mpad;
+  std::vector<double> h((size_t)M * M);
+  CTC_CUDA_TRY(cudaMemcpyAsync(h.data(), d_D, sizeof(double) * M * M, cudaMemcpyDeviceToHost, st));
+  CTC_CUDA_TRY(cudaStreamSynchronize(st));
+  std::vector<double> pad((size_t)Mp * Mp, 0.0);
+  for (int i = 0; i < M; ++i) {
+    const double* src = &h[(size_t)m->ao_perm[i] * M];
+    for (int j = 0; j < M; ++j) {
+      const double v = src[m->ao_perm[j]];
+      m->D[(size_t)i * M + j] = v;
+      pad[(size_t)i * Mp + j] = v;
+    }
+  }
+  CTC_CUDA_TRY(cudaMemcpyAsync(m->d_D, pad.data(), sizeof(double) * pad.size(), cudaMemcpyHostToDevice, st));
   CTC_CUDA_TRY(cudaStreamSynchronize(st));
   m->dsl_valid = false;
   m->esp_valid = false;

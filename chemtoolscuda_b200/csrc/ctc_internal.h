@@ -37,10 +37,12 @@ struct DevSeg {
   int32_t l;
   int32_t nprim;
   int32_t prim0;    // first primitive in the primitive arrays
-  int32_t ao0;      // first AO index
+  int32_t ao0;      // first AO index (internal, spatially sorted order)
   int32_t atom;     // owning atom or -1
+  int32_t orig_ao0; // first AO index in the caller's order
+  int32_t pad;
 };
-static_assert(sizeof(DevSeg) == 56 || sizeof(DevSeg) == 64, "DevSeg layout");
+static_assert(sizeof(DevSeg) == 64, "DevSeg layout");
 
 // Polynomial term of one AO component: coef * x^a y^b z^c (angular normalisation folded in).
 struct Term {
@@ -117,7 +119,9 @@ struct ctc_molecule {
   std::vector<int32_t> seg_order;            // segments sorted by type, nprim
   std::vector<double> atom_xyz, charges;
   std::vector<double> D;                     // host copy, M x M
-  std::vector<int32_t> ao_atom;              // AO -> atom
+  std::vector<int32_t> ao_atom;              // AO -> atom (internal order)
+  std::vector<int32_t> ao_perm;              // internal AO -> caller's AO
+  int32_t* d_ao_iperm = nullptr;             // caller's AO -> internal AO
   // device tables
   ctc::DevSeg* d_segs = nullptr;
   double* d_alpha = nullptr;

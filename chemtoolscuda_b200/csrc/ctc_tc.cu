@@ -207,34 +207,43 @@ __global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint32_t*
     Dp[(int64_t)row * Mpad + k] = pack_digits(to_fixed(d[k], e));
 }
 
-// Tile A rows (FP64, compact K) -> four int8 planes [t][plane][row][Kcap] and row exponents.
+// Tile A rows (FP64, compact K, block layout [q][k][point]) -> four int8
+// planes [t][plane][row][Kcap] (row = q * PTS + point, K contiguous) and row
+// exponents.  Each lane owns one row: the row maximum reads consecutive points
+// across lanes, and every lane then writes 32 bytes per plane per step.
 __global__ void slice_a_kernel(TileBatch tb, int nqa, int8_t* __restrict__ planes,
                                int32_t* __restrict__ eexp) {
   const int t = blockIdx.x;
   const int kt = tb.kt[t];
   const int PTS = kRows / nqa;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t ldq = (int64_t)tb.TP * tb.Kcap;
+  const int64_t ldq = (int64_t)PTS * tb.Kcap;
   const double* A = tb.ao + (int64_t)t * tb.nq * ldq;
   int8_t* P = planes + (int64_t)t * kPlanes * kRows * tb.Kcap;
-  for (int r = warp; r < kRows; r += blockDim.x >> 5) {
+  for (int r = warp * 32 + lane; r < kRows; r += blockDim.x) {
     const int q = r / PTS, pl = r % PTS;
-    const double* row = A + q * ldq + (int64_t)pl * tb.Kcap;
+    const double* col = A + q * ldq + pl;  // element k at col[k * PTS]
     double m = 0.0;
-    for (int k = lane; k < kt; k += 32) m = fmax(m, fabs(row[k]));
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    for (int k = 0; k < kt; ++k) m = fmax(m, fabs(col[(int64_t)k * PTS]));
     const int e = scale_exponent(m);
-    if (lane == 0) eexp[(int64_t)t * kRows + r] = e;
-    for (int k4 = lane * 4; k4 < kt; k4 += 128) {
-      uint32_t w[4];
+    eexp[(int64_t)t * kRows + r] = e;
+    for (int k0 = 0; k0 < kt; k0 += 32) {
+      uint32_t pw[kPlanes][8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) w[i] = pack_digits(to_fixed(row[k4 + i], e));
+      for (int g = 0; g < 8; ++g) {
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = pack_digits(to_fixed(col[(int64_t)(k0 + 4 * g + i) * PTS], e));
+#pragma unroll
+        for (int p = 0; p < kPlanes; ++p)
+          pw[p][g] = ((w[0] >> (8 * p)) & 255) | (((w[1] >> (8 * p)) & 255) << 8) |
+                     (((w[2] >> (8 * p)) & 255) << 16) | (((w[3] >> (8 * p)) & 255) << 24);
+      }
 #pragma unroll
       for (int p = 0; p < kPlanes; ++p) {
-        // byte p of each word -> 4 consecutive bytes of plane p
-        const uint32_t out = ((w[0] >> (8 * p)) & 255) | (((w[1] >> (8 * p)) & 255) << 8) |
-                             (((w[2] >> (8 * p)) & 255) << 16) | (((w[3] >> (8 * p)) & 255) << 24);
-        *(uint32_t*)(P + ((int64_t)p * kRows + r) * tb.Kcap + k4) = out;
+        uint4* dst = reinterpret_cast<uint4*>(P + ((int64_t)p * kRows + r) * tb.Kcap + k0);
+        dst[0] = make_uint4(pw[p][0], pw[p][1], pw[p][2], pw[p][3]);
+        dst[1] = make_uint4(pw[p][4], pw[p][5], pw[p][6], pw[p][7]);
       }
     }
   }
@@ -401,7 +410,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     const int q = r / PTS, pl = r % PTS;
     const int nq_ao = tb.nq;
     const int64_t ldq = (int64_t)tb.TP * tb.Kcap;
-    const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + (int64_t)pl * tb.Kcap;
+    const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pl;  // element (q, k) at aop[q*ldq + k*PTS]
     const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 60);
     // quantities this row is reduced against: q = 0 -> phi, d phi, d2 phi; q = k -> d_j phi, j >= k
     const int qa = (q == 0) ? 0 : q;
@@ -438,13 +447,13 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         for (int j = 0; j < 16; ++j) g[j] *= rowscale * cs[c * 16 + j];
         const int col = n0 + c * 16;
         for (int qq = qa; qq < qb; ++qq) {
-          const double2* src = reinterpret_cast<const double2*>(aop + qq * ldq + col);
-          double2 v2[8];
+          const double* src = aop + qq * ldq + (int64_t)col * PTS;
+          double v[16];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) v2[j] = __ldg(src + j);
+          for (int j = 0; j < 16; ++j) v[j] = __ldg(src + j * PTS);
           double acc = 0.0;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc += g[2 * j] * v2[j].x + g[2 * j + 1] * v2[j].y;
+          for (int j = 0; j < 16; ++j) acc += g[j] * v[j];
           sums[qq - qa] += acc;
         }
       }

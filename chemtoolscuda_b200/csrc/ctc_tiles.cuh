@@ -249,10 +249,10 @@ __global__ void __launch_bounds__(kTileThreads)
 
 // ------------------------------------------------------------------ FP64 contraction kernel
 constexpr int BM = 128, BN = 64, BK = 32, STAGES = 3;
-constexpr int A_LD = BK + 4;  // 36 doubles: conflict-free fragment loads
+constexpr int A_LD = BM + 4;  // A stage stored [k][row], 132 doubles: conflict-free fragment loads
 constexpr int B_LD = BN + 4;  // 68 doubles
 constexpr int C_LD = BN + 1;
-constexpr int A_STAGE = BM * A_LD, B_STAGE = BK * B_LD;
+constexpr int A_STAGE = BK * A_LD, B_STAGE = BK * B_LD;
 constexpr int kThreads = 256;
 constexpr size_t kSmemPipe = sizeof(double) * STAGES * (A_STAGE + B_STAGE);
 constexpr size_t kSmemC = sizeof(double) * BM * C_LD;
@@ -320,7 +320,9 @@ __global__ void __launch_bounds__(kThreads)
   const double* A = tb.ao + (int64_t)t * nq_ao * ldq;
   const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
 
-  const int epl = tid / TPP, esub = tid % TPP;
+  // epilogue ownership: lanes take consecutive points (coalesced AO reads),
+  // esub selects the column subset; partial sums meet in shared memory
+  const int epl = tid % PTS, esub = tid / PTS;
   double acc_s[NS];
 #pragma unroll
   for (int i = 0; i < NS; ++i) acc_s[i] = 0.0;
@@ -351,12 +353,13 @@ __global__ void __launch_bounds__(kThreads)
       double* a = sA + stage * A_STAGE;
       double* b = sB + stage * B_STAGE;
       const int k0 = kb * BK;
+      // A stage [k][row]: 32 k x 128 rows, each (q, k) a run of PTS points
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int ch = tid + i * kThreads;
-        const int r = ch >> 4, cc = (ch & 15) * 2;
+        const int kk = ch >> 6, r = (ch & 63) * 2;
         const int q = r / PTS, pl = r % PTS;
-        cp_async16(a + r * A_LD + cc, A + q * ldq + (int64_t)pl * tb.Kcap + k0 + cc, true);
+        cp_async16(a + kk * A_LD + r, A + q * ldq + (int64_t)(k0 + kk) * PTS + pl, true);
       }
       // B gather: 32 rows (compact mu) x 64 columns (compact nu), 8 bytes each
 #pragma unroll
@@ -385,7 +388,7 @@ __global__ void __launch_bounds__(kThreads)
         double af[4], bf[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          af[i] = a[(wm * 32 + i * 8 + (lane >> 2)) * A_LD + ks + (lane & 3)];
+          af[i] = a[(ks + (lane & 3)) * A_LD + wm * 32 + i * 8 + (lane >> 2)];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           bf[j] = b[(ks + (lane & 3)) * B_LD + wn * 32 + j * 8 + (lane >> 2)];
@@ -410,13 +413,14 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     if constexpr (EPI == 0) {
       {
-        const double* aop = A + (int64_t)epl * tb.Kcap + n0;
+        // AO value of quantity q at column n0 + v for this point: A[q][n0 + v][epl]
+        const double* aop = A + (int64_t)n0 * PTS + epl;
         for (int v = esub; v < BN; v += TPP) {
           const double G0 = sC[(0 * PTS + epl) * C_LD + v];
-          const double phi = aop[v];
+          const double phi = aop[v * PTS];
           acc_s[0] += G0 * phi;
           if (nq_ao >= 4) {
-            const double d0 = aop[ldq + v], d1 = aop[2 * ldq + v], d2 = aop[3 * ldq + v];
+            const double d0 = aop[ldq + v * PTS], d1 = aop[2 * ldq + v * PTS], d2 = aop[3 * ldq + v * PTS];
             acc_s[1] += G0 * d0;
             acc_s[2] += G0 * d1;
             acc_s[3] += G0 * d2;
@@ -432,7 +436,7 @@ __global__ void __launch_bounds__(kThreads)
               acc_s[15] += G3 * d2;
               if (nq_ao == 10) {
   #pragma unroll
-                for (int h = 0; h < 6; ++h) acc_s[4 + h] += G0 * aop[(4 + h) * ldq + v];
+                for (int h = 0; h < 6; ++h) acc_s[4 + h] += G0 * aop[(4 + h) * ldq + v * PTS];
               }
             }
           }
@@ -441,7 +445,7 @@ __global__ void __launch_bounds__(kThreads)
     } else {
       // dL/dR_A,j += sum over nu on atom A of
       //   -2 v_rho d_j phi G0 - 2 sum_k v_k (d_j d_k phi G0 + d_j phi G_k)
-      const double* aop = A + (int64_t)epl * tb.Kcap + n0;
+      const double* aop = A + (int64_t)n0 * PTS + epl;
       const int hidx[3][3] = {{4, 5, 6}, {5, 7, 8}, {6, 8, 9}};
       for (int v = esub; v < BN; v += TPP) {
         const int nu = s_colmap[v];
@@ -456,11 +460,11 @@ __global__ void __launch_bounds__(kThreads)
           Gk[2] = sC[(3 * PTS + epl) * C_LD + v];
         }
         for (int j = 0; j < 3; ++j) {
-          const double dj = aop[(1 + j) * ldq + v];
+          const double dj = aop[(1 + j) * ldq + v * PTS];
           double c = -2.0 * fvr * dj * G0;
           if (fa.v_grad) {
             for (int k = 0; k < 3; ++k)
-              c -= 2.0 * fvg[k] * (aop[hidx[j][k] * ldq + v] * G0 + dj * Gk[k]);
+              c -= 2.0 * fvg[k] * (aop[hidx[j][k] * ldq + v * PTS] * G0 + dj * Gk[k]);
           }
           if (force_smem) atomicAdd(&s_force[3 * atom + j], c);
           else atomicAdd(&fa.dLdR[3 * atom + j], c);
@@ -476,16 +480,21 @@ __global__ void __launch_bounds__(kThreads)
         if (s_force[i] != 0.0) atomicAdd(&fa.dLdR[i], s_force[i]);
     return;
   }
+  // sum the TPP column subsets of each point (sC is free after the last tile)
+  double* red = sC;
 #pragma unroll
-  for (int i = 0; i < NS; ++i)
-#pragma unroll
-    for (int off = TPP / 2; off > 0; off >>= 1)
-      acc_s[i] += __shfl_xor_sync(0xffffffffu, acc_s[i], off);
+  for (int i = 0; i < NS; ++i) red[(esub * NS + i) * PTS + epl] = acc_s[i];
+  __syncthreads();
   const int64_t oidx = tb.out[(int64_t)t * PTS + epl];
   if (esub == 0 && oidx >= 0) {
     double s[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) s[i] = i < NS ? acc_s[i] : 0.0;
+    for (int i = 0; i < 16; ++i) {
+      double v = 0.0;
+      if (i < NS)
+        for (int e = 0; e < TPP; ++e) v += red[(e * NS + i) * PTS + epl];
+      s[i] = v;
+    }
     finalize_point(s, NQA, nq_ao, out, oidx, prm);
   }
 }

@@ -2,7 +2,7 @@
 
 For every segment type (s, p, Cartesian/pure d, f, g) one device function
 evaluates all components and, depending on DERIV, their first and second
-derivatives, given powers X[i] = x^(i-2) (X[0] = X[1] = 0), the same for y and
+derivatives (written to o[q * ld_q + component * ldc]), given powers X[i] = x^(i-2) (X[0] = X[1] = 0), the same for y and
 z, and the contracted radial sums R0, R1, R2 (see ctc_ao.cu).  The terms come
 from gen_terms.py; writing their exponents as literals lets the compiler keep
 the power arrays in registers.
@@ -21,7 +21,7 @@ def emit_type(ti, l, pure):
     out = [f"// type {ti}: l = {l}{' (pure)' if pure else ''}, {len(cs)} components",
            "template <int DERIV>",
            f"__device__ __forceinline__ void ao_poly_{ti}(const double* X, const double* Y, const double* Z,",
-           "    double R0, double R1, double R2, double* __restrict__ o, int64_t ld_q, int nq_out) {"]
+           "    double R0, double R1, double R2, double* __restrict__ o, int64_t ld_q, int64_t ldc, int nq_out) {"]
     for j, comp in enumerate(cs):
         out.append("  {")
         out.append("    double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0, q4 = 0.0, q5 = 0.0, q6 = 0.0, q7 = 0.0, q8 = 0.0, q9 = 0.0;")
@@ -42,10 +42,11 @@ def emit_type(ti, l, pure):
             out.append(f"        q9 += {C} * X[{a+2}] * Y[{b+2}] * ({z*(z-1)}.0 * Z[{z}] * R0 - {2*(2*z+1)}.0 * Z[{z+2}] * R1 + 4.0 * Z[{z+4}] * R2);")
             out.append("      }")
             out.append("    }")
-        out.append(f"    o[{j}] = q0;")
-        out.append(f"    if (DERIV >= 1) {{ if (nq_out > 1) {{ o[ld_q + {j}] = q1; o[2 * ld_q + {j}] = q2; o[3 * ld_q + {j}] = q3; }} }}")
-        out.append(f"    if (DERIV >= 2) {{ if (nq_out > 4) {{ o[4 * ld_q + {j}] = q4; o[5 * ld_q + {j}] = q5; o[6 * ld_q + {j}] = q6;")
-        out.append(f"      o[7 * ld_q + {j}] = q7; o[8 * ld_q + {j}] = q8; o[9 * ld_q + {j}] = q9; }} }}")
+        c = f"{j} * ldc"
+        out.append(f"    o[{c}] = q0;")
+        out.append(f"    if (DERIV >= 1) {{ if (nq_out > 1) {{ o[ld_q + {c}] = q1; o[2 * ld_q + {c}] = q2; o[3 * ld_q + {c}] = q3; }} }}")
+        out.append(f"    if (DERIV >= 2) {{ if (nq_out > 4) {{ o[4 * ld_q + {c}] = q4; o[5 * ld_q + {c}] = q5; o[6 * ld_q + {c}] = q6;")
+        out.append(f"      o[7 * ld_q + {c}] = q7; o[8 * ld_q + {c}] = q8; o[9 * ld_q + {c}] = q9; }} }}")
         out.append("  }")
     out.append("}")
     return out
