@@ -56,7 +56,7 @@ def case_allshell():
 
 
 def case_c1():
-    """The first benchmark configuration's generator (12 atoms, Cartesian up to d)."""
+    """The 12-atom synthetic molecule (Cartesian shells up to d, ~120 functions)."""
     mol = S.make_molecule("c1", seed=7)
     rng = np.random.default_rng(12)
     pts = S.random_points(rng, mol, 256)

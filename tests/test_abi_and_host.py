@@ -36,7 +36,7 @@ REFERENCE_BOUND = [  # src/pybind.cpp:15-304
     "compute_gradient_expansion_ked", "compute_empirical_gradient_expansion_ked",
     "compute_general_ked", "compute_schrodinger_ked", "compute_shannon_information_density",
     "compute_electrostatic_potential", "coordinates", "numbers", "get_file_path"]
-README_NAMES = [  # names used by the reference's README/tests and north star
+README_NAMES = [  # names used by the reference's README and tests
     "compute_electron_density", "compute_electron_density_gradient",
     "compute_electron_density_hessian", "compute_laplacian_electron_density",
     "compute_electron_density_on_cubic_grid", "basis_set_to_constant_memory",

@@ -2,9 +2,8 @@
 
 * dL/dD and dL/dR through the C ABI against the FP64 oracle (1e-10 relative);
 * the autograd path on L = sum_g w_g (c1 rho^(4/3) + c2 |grad rho|^2 / rho^(4/3))
-  against FP64 central finite differences (h = 1e-5) on 20 random D entries
-  and all coordinates -- tolerance 1e-6 relative to the largest gradient entry,
-  the north-star bound;
+  against FP64 central finite differences (h = 1e-5) on 20 random symmetric
+  pairs of D entries and all coordinates -- tolerance 1e-6 relative to the largest gradient entry;
 * the translational sum rule sum_A dL/dR_A = -sum_g (v_rho grad rho + H v_grad).
 """
 import numpy as np
@@ -77,12 +76,18 @@ def test_autograd_vs_finite_differences(torch_cuda):
     M = mol.nbasis
     idx = [(int(a), int(b)) for a, b in rng.integers(0, M, size=(20, 2))]
     fdD = []
+    # D stays symmetric under the perturbation (the forward formulas, like the
+    # reference's, assume a symmetric density matrix): moving D[a,b] and D[b,a]
+    # together measures dL/dD[a,b] + dL/dD[b,a] (once for a == b).
     with torch.no_grad():
         for (a, b) in idx:
             Dp = D.detach().clone()
-            Dp[a, b] += h
             Dm = D.detach().clone()
+            Dp[a, b] += h
             Dm[a, b] -= h
+            if a != b:
+                Dp[b, a] += h
+                Dm[b, a] -= h
             fdD.append((L(Dp, R.detach()).item() - L(Dm, R.detach()).item()) / (2 * h))
         fdR = np.zeros_like(gR)
         for A in range(len(mol.coords)):
@@ -92,7 +97,7 @@ def test_autograd_vs_finite_differences(torch_cuda):
                 Rm = R.detach().clone()
                 Rm[A, j] -= h
                 fdR[A, j] = (L(D.detach(), Rp).item() - L(D.detach(), Rm).item()) / (2 * h)
-    an = np.array([gD[a, b] for (a, b) in idx])
+    an = np.array([gD[a, b] + (gD[b, a] if a != b else 0.0) for (a, b) in idx])
     scaleD = max(np.abs(gD).max(), 1e-30)
     assert np.abs(an - np.array(fdD)).max() <= 1e-6 * scaleD, (an, fdD)
     scaleR = max(np.abs(gR).max(), 1e-30)

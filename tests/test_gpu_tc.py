@@ -3,8 +3,8 @@ operands, exact int32 accumulation) against the FP64 oracle.
 
 Stated tolerance: 1e-8 relative to the per-point sum of absolute terms
 (tests/helpers.py) for rho, grad rho, Hessian, Laplacian, tau_PD and
-tau_alpha -- the north-star bound; the scheme's measured error on the
-200-atom molecule is ~2e-9."""
+tau_alpha -- the accuracy bound the split path is built to; its measured
+error on the 200-atom molecule is ~2e-9."""
 import os
 
 import numpy as np
