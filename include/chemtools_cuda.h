@@ -124,6 +124,20 @@ int ctc_molecule_prepare(ctc_molecule* mol, int32_t precision);
 int ctc_eval_local(ctc_molecule* mol, const double* d_points, int64_t npoints, int32_t precision,
                    const ctc_params* params, const ctc_outputs* d_out, void* stream);
 
+/* ctc_eval_local in the FP64 form for callers that cannot allocate device
+ * memory during a call (a caller whose own arena holds the device's memory,
+ * a run that allocates only at start-up, a process under a fixed
+ * device-memory quota).  Has no counterpart in the reference.  It allocates
+ * nothing: its scratch is one 64 MiB array compiled into the library, held on
+ * every GPU that loads it until the process exits.  At most 1,048,576 points
+ * per call, and a basis whose AO block for one 32-point tile does not fit
+ * the array is refused; both return CTC_ERR_INVALID with the limit in
+ * ctc_last_error().  The first call on a device looks up the array's device
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race, so serialise them on one stream. */
+int ctc_eval_local_noalloc(ctc_molecule* mol, const double* d_points, int64_t npoints,
+                           const ctc_params* params, const ctc_outputs* d_out, void* stream);
+
 /* Same with host points and host outputs; copies are inside the call. */
 int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t npoints,
                         int32_t precision, const ctc_params* params, const ctc_outputs* h_out);
