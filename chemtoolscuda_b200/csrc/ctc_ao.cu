@@ -18,6 +18,7 @@
 // (every value and derivative below 1e-18) writes zeros without evaluating
 // exponentials.  Arithmetic is FP64 throughout.
 #include "ctc_internal.h"
+#include "ctc_split.cuh"
 
 #include "ctc_terms.inc"
 
@@ -128,16 +129,22 @@ __global__ void __launch_bounds__(kAoThreads)
   }
 }
 
+// High 32 bits of |x| (sign cleared): ordered like |x|, and bits 20..30 hold
+// the biased exponent.
+__device__ __forceinline__ unsigned abs_hi(double x) {
+  return (unsigned)__double2hiint(x) & 0x7fffffffu;
+}
+
 #include "ctc_ao_poly.inc"
 
 // Type-specialised evaluation of one segment at one point: the polynomial
 // code of every component has literal exponents (ctc_ao_poly.inc), so the
 // powers stay in registers.  Same arithmetic as eval_segment.
-template <int DERIV, int TYPE>
+template <int DERIV, int TYPE, int TRACK>
 __device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __restrict__ alpha,
                                            const double* __restrict__ coef, double px, double py,
                                            double pz, double* __restrict__ o, int64_t ld_q,
-                                           int64_t ldc, int nq_out) {
+                                           int64_t ldc, int nq_out, unsigned* mx) {
   constexpr int L = TYPE == 0 ? 0 : (TYPE == 1 ? 1 : (TYPE <= 3 ? 2 : (TYPE <= 5 ? 3 : 4)));
   constexpr int NC = TYPE == 0 ? 1 : TYPE == 1 ? 3 : TYPE == 2 ? 6 : TYPE == 3 ? 5
                      : TYPE == 4 ? 10 : TYPE == 5 ? 7 : TYPE == 6 ? 15 : 9;
@@ -167,30 +174,30 @@ __device__ __forceinline__ void eval_typed(const DevSeg& sg, const double* __res
     Y[i] = Y[i - 1] * y;
     Z[i] = Z[i - 1] * z;
   }
-  if constexpr (TYPE == 0) ao_poly_0<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 1) ao_poly_1<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 2) ao_poly_2<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 3) ao_poly_3<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 4) ao_poly_4<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 5) ao_poly_5<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else if constexpr (TYPE == 6) ao_poly_6<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
-  else ao_poly_7<DERIV>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out);
+  if constexpr (TYPE == 0) ao_poly_0<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 1) ao_poly_1<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 2) ao_poly_2<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 3) ao_poly_3<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 4) ao_poly_4<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 5) ao_poly_5<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else if constexpr (TYPE == 6) ao_poly_6<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
+  else ao_poly_7<DERIV, TRACK>(X, Y, Z, R0, R1, R2, o, ld_q, ldc, nq_out, mx);
 }
 
-template <int DERIV>
+template <int DERIV, int TRACK>
 __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __restrict__ alpha,
                                               const double* __restrict__ coef, double px, double py,
                                               double pz, double* __restrict__ o, int64_t ld_q,
-                                              int64_t ldc, int nq_out) {
+                                              int64_t ldc, int nq_out, unsigned* mx) {
   switch (sg.type) {
-    case 0: eval_typed<DERIV, 0>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 1: eval_typed<DERIV, 1>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 2: eval_typed<DERIV, 2>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 3: eval_typed<DERIV, 3>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 4: eval_typed<DERIV, 4>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 5: eval_typed<DERIV, 5>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    case 6: eval_typed<DERIV, 6>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
-    default: eval_typed<DERIV, 7>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out); break;
+    case 0: eval_typed<DERIV, 0, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 1: eval_typed<DERIV, 1, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 2: eval_typed<DERIV, 2, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 3: eval_typed<DERIV, 3, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 4: eval_typed<DERIV, 4, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 5: eval_typed<DERIV, 5, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    case 6: eval_typed<DERIV, 6, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
+    default: eval_typed<DERIV, 7, TRACK>(sg, alpha, coef, px, py, pz, o, ld_q, ldc, nq_out, mx); break;
   }
 }
 
@@ -199,10 +206,19 @@ __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __
 // and its stores of one (quantity, AO) cover consecutive points.  Layout of
 // the tile block: A[q][k][point] (point fastest).  Padding columns
 // [ktrue, kt) are zeroed.
-template <int DERIV>
+//
+// SLICE = 4 or 1 also produces the row exponents of the tensor-core split
+// operands of the tile (ctc_split.cuh): the rows are 32 points x {phi, d_x,
+// d_y, d_z phi} (SLICE = 4, row = q * 32 + point) or 128 points x phi
+// (SLICE = 1).  Every lane keeps the running maximum of its values while it
+// evaluates, so the exponents cost no second pass over the block;
+// slice_rows_kernel then writes the digit planes.
+template <int DERIV, int SLICE>
 __global__ void __launch_bounds__(kAoThreads, 3)
     ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
-                   const double* __restrict__ coef, TileBatch tb) {
+                   const double* __restrict__ coef, TileBatch tb, int32_t* __restrict__ eexp) {
+  // per-warp maxima of the high word of |value| per row, [warp][row]
+  __shared__ unsigned s_mx[SLICE ? kAoThreads / 32 : 1][SLICE ? kSplitRows : 1];
   const int t = blockIdx.x;
   const int ns = tb.nsig[t], TP = tb.TP;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -214,9 +230,17 @@ __global__ void __launch_bounds__(kAoThreads, 3)
   for (int pg = 0; pg < TP; pg += 32) {
     const int j = pg + lane;
     const double px = xyz[3 * j], py = xyz[3 * j + 1], pz = xyz[3 * j + 2];
+    unsigned mx[4] = {0u, 0u, 0u, 0u};
     for (int i = warp; i < ns; i += kAoThreads / 32) {
       const DevSeg sg = segs[sl[i]];
-      eval_dispatch<DERIV>(sg, alpha, coef, px, py, pz, A + (int64_t)k0[i] * TP + j, ld_q, TP, tb.nq);
+      eval_dispatch<DERIV, SLICE>(sg, alpha, coef, px, py, pz, A + (int64_t)k0[i] * TP + j, ld_q, TP,
+                                  tb.nq, mx);
+    }
+    if (SLICE == 4) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s_mx[SLICE ? warp : 0][SLICE ? q * 32 + lane : 0] = mx[q];
+    } else if (SLICE == 1) {
+      s_mx[SLICE ? warp : 0][SLICE ? j : 0] = mx[0];
     }
   }
   const int kt_true = tb.ktrue[t], kt = tb.kt[t];
@@ -224,6 +248,47 @@ __global__ void __launch_bounds__(kAoThreads, 3)
   for (int idx = threadIdx.x; idx < tb.nq * npad; idx += kAoThreads) {
     const int q = idx / npad, r = idx % npad;
     A[q * ld_q + (int64_t)kt_true * TP + r] = 0.0;
+  }
+  if (SLICE != 0) {
+    __syncthreads();  // row maxima of every warp are in shared memory
+    const int r = threadIdx.x;  // one row per thread (kAoThreads == kSplitRows)
+    unsigned m = 0u;
+#pragma unroll
+    for (int w = 0; w < kAoThreads / 32; ++w) m = max(m, s_mx[SLICE ? w : 0][SLICE ? r : 0]);
+    // |x| = 1.f 2^(E - 1023) < 2^(E - 1022) for the biased exponent E of the
+    // largest |x| (frexp's exponent); a row of zeros gets 0
+    const int E = (int)(m >> 20);
+    const int e = m == 0u ? 0 : E - 1022;
+    eexp[(int64_t)t * kSplitRows + r] = e < kMinScaleExponent ? kMinScaleExponent : e;
+  }
+}
+
+// Digit planes of the tile rows (ctc_split.cuh) with the exponents found by
+// ao_tile_kernel.  Work items are (32-row group, 32-column chunk): a warp
+// reads one 256-byte line per column (32 consecutive rows = points of one
+// quantity) and each lane writes 32 bytes per plane of its own row.
+constexpr int kSliceThreads = 256;
+
+__global__ void __launch_bounds__(kSliceThreads)
+    slice_rows_kernel(TileBatch tb, int nqa, const int32_t* __restrict__ eexp,
+                      int8_t* __restrict__ planes) {
+  const int t = blockIdx.x;
+  const int kt = tb.kt[t];
+  const int TP = tb.TP;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t ld_q = (int64_t)TP * tb.Kcap;
+  const double* A = tb.ao + (int64_t)t * tb.nq * ld_q;
+  int8_t* P = planes + (int64_t)t * kSplitPlanes * kSplitRows * tb.Kcap;
+  const int nchunk = kt / 32;
+  const int nitem = (kSplitRows / 32) * nchunk;  // warp-sized items
+  for (int it = warp; it < nitem; it += kSliceThreads / 32) {
+    const int rg = it % (kSplitRows / 32), c = it / (kSplitRows / 32);
+    const int r = rg * 32 + lane;
+    const int q = nqa == 4 ? rg : 0;
+    const int p = nqa == 4 ? lane : r;
+    const double f = split_row_factor(eexp[(int64_t)t * kSplitRows + r]);
+    const double* col = A + q * ld_q + p + (int64_t)(c * 32) * TP;
+    write_row_digits32([&](int i) { return __ldg(col + (int64_t)i * TP); }, f, P, r, tb.Kcap, c * 32);
   }
 }
 
@@ -265,11 +330,37 @@ int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv
 
 int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
+  const auto* sg = mol->d_segs;
   switch (deriv) {
-    case 0: ao_tile_kernel<0><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb); break;
-    case 1: ao_tile_kernel<1><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb); break;
-    default: ao_tile_kernel<2><<<tb.C, kAoThreads, 0, st>>>(mol->d_segs, mol->nseg, mol->d_alpha, mol->d_coef, tb);
+    case 0: ao_tile_kernel<0, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr); break;
+    case 1: ao_tile_kernel<1, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr); break;
+    default: ao_tile_kernel<2, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr);
   }
+  CTC_CUDA_TRY(cudaGetLastError());
+  return CTC_OK;
+}
+
+int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
+                           int8_t* planes, int32_t* eexp, cudaStream_t st) {
+  if (tb.C <= 0) return CTC_OK;
+  if (!(nqa == 4 && tb.TP == 32 && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
+    return fail(CTC_ERR_INVALID, "sliced AO tiles: unsupported row layout");
+  if (planes == nullptr || eexp == nullptr)
+    return fail(CTC_ERR_INVALID, "sliced AO tiles: null workspace");
+  const auto* sg = mol->d_segs;
+  const double *al = mol->d_alpha, *co = mol->d_coef;
+  if (nqa == 4) {
+    if (deriv == 1) ao_tile_kernel<1, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
+    else ao_tile_kernel<2, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
+  } else {
+    switch (deriv) {
+      case 0: ao_tile_kernel<0, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp); break;
+      case 1: ao_tile_kernel<1, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp); break;
+      default: ao_tile_kernel<2, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
+    }
+  }
+  CTC_CUDA_TRY(cudaGetLastError());
+  slice_rows_kernel<<<tb.C, kSliceThreads, 0, st>>>(tb, nqa, eexp, planes);
   CTC_CUDA_TRY(cudaGetLastError());
   return CTC_OK;
 }

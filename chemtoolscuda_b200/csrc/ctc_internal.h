@@ -152,6 +152,12 @@ namespace ctc {
 // ---- kernels / launchers (ctc_ao.cu) ----
 // AO block of every tile of a batch on its significant segments only.
 int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cudaStream_t st);
+// Same, and in the same kernel the int8 digit planes of the tile rows
+// (nqa = 4: 32 points x {phi, d phi}; nqa = 1: 128 points x phi) with one
+// exponent per row, for the tensor-core split path: planes [C][4][128][Kcap],
+// eexp [C][128].
+int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
+                           int8_t* planes, int32_t* eexp, cudaStream_t st);
 int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
               int nq_out, int ld, cudaStream_t st);
 // AO output in (nq, n, M) layout for ctc_eval_ao.
@@ -170,6 +176,9 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
 
 // ---- tensor-core split path (ctc_tc.cu) ----
 int prepare_tc(ctc_molecule* mol, cudaStream_t st);
+// Workspace of the digit planes and row exponents of a chunk of tiles.
+int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
+                       int32_t** eexp);
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
 

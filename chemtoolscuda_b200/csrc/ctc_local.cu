@@ -76,18 +76,28 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
     if (rc != CTC_OK) return rc;
   }
   const int TP = 128 / plan.nqa;
-  int rc = run_tiles(mol, src, n, TP, plan.nq_ao, plan.deriv, st, [&](const TileBatch& tb) {
-    int r;
-    if (precision == CTC_PREC_FP64) {
-      ProfScope ps(mol, 0, st);
-      r = fp64_local_tiles(mol, plan, tb, prm, out, st);
-      mol->host_launches += 1;
-    } else {
-      r = tc_local_tiles(mol, plan, tb, prm, out, st);
-      mol->host_launches += 2;  // operand slicing + contraction
-    }
-    return r;
-  });
+  // tensor-core path: the AO kernel also writes the int8 digit planes
+  const std::function<int(const TileBatch&)> sliced_ao = [&](const TileBatch& tb) {
+    int8_t* planes = nullptr;
+    int32_t* eexp = nullptr;
+    int r = tc_slice_workspace(mol, tb, st, &planes, &eexp);
+    if (r != CTC_OK) return r;
+    return launch_ao_tiles_sliced(mol, tb, plan.deriv, plan.nqa, planes, eexp, st);
+  };
+  int rc = run_tiles(
+      mol, src, n, TP, plan.nq_ao, plan.deriv, st,
+      [&](const TileBatch& tb) {
+        int r;
+        if (precision == CTC_PREC_FP64) {
+          ProfScope ps(mol, 0, st);
+          r = fp64_local_tiles(mol, plan, tb, prm, out, st);
+        } else {
+          r = tc_local_tiles(mol, plan, tb, prm, out, st);
+        }
+        mol->host_launches += 1;
+        return r;
+      },
+      precision == CTC_PREC_TC_SPLIT ? &sliced_ao : nullptr);
   if (rc != CTC_OK) return rc;
   // the tensor-core kernels report bounded-wait timeouts through the status word
   if (precision == CTC_PREC_TC_SPLIT) return check_status(mol, st, "tensor-core contraction");

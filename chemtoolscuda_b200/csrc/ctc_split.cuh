@@ -1,0 +1,91 @@
+// ctc_split.cuh -- the INT8 digit split shared by the operand producers
+// (D in ctc_tc.cu, the tile rows in the AO kernel of ctc_ao.cu).
+//
+// A row of values x_k (a tile row of phi or d_k phi over the tile's compact
+// AOs, or a row of D) is scaled by 2^-e, e the exponent of its largest |x|
+// (|x| < 2^e), and rounded to the 31-bit fixed-point integer
+// I = rint(x 2^(30-e)), |I| <= 2^30.  I is written as four balanced base-256
+// digits d_0..d_3, |d_i| <= 128, I = sum_i d_i 256^(3-i): one int8 plane per
+// digit, most significant first.
+#pragma once
+
+#include <cstdint>
+
+namespace ctc {
+
+constexpr int kSplitPlanes = 4;   // digit planes per operand
+constexpr int kSplitRows = 128;   // rows of a tile operand (MMA M)
+
+// Lowest row exponent used: rows whose largest |x| is below 2^-990 are
+// scaled as if it were 2^-990 (their digits are then zero), so that the row
+// factor 2^(30 - e) stays a normal double.
+constexpr int kMinScaleExponent = -990;
+
+// balanced base-256 digits of |I| <= 2^30, packed in a word: byte p holds the
+// digit of weight 256^(3-p) (byte 0 = the most significant digit).  Adding
+// 128 (256^2 + 256 + 1) turns the three low balanced digits d into unsigned
+// bytes d + 128 and leaves the top digit in the high byte; flipping bit 7 of
+// the low bytes gives d as int8, and a byte reversal puts the most
+// significant digit first.
+__device__ __forceinline__ uint32_t pack_digits(int32_t I) {
+  const uint32_t u = (uint32_t)(I + 0x808080) ^ 0x808080u;
+  return __byte_perm(u, 0u, 0x0123);
+}
+
+// rint(y) for |y| < 2^31 (round half to even) with one FP64 add: the sum
+// y + 1.5 * 2^52 has unit spacing, so its low word is rint(y) mod 2^32.
+__device__ __forceinline__ int32_t rint_i32(double y) {
+  return __double2loint(y + 6755399441055744.0);
+}
+
+// 2^(30 - e): the factor that maps a row with |x| < 2^e onto |I| <= 2^30
+__device__ __forceinline__ double split_row_factor(int e) {
+  return __longlong_as_double((long long)(30 - e + 1023) << 52);
+}
+
+__device__ __forceinline__ int scale_exponent(double amax) {
+  if (!(amax > 0.0)) return 0;
+  int e;
+  frexp(amax, &e);  // amax = m 2^e, m in [0.5, 1)
+  return e < kMinScaleExponent ? kMinScaleExponent : e;
+}
+
+// 4 x 4 byte transpose: out[p] byte j = byte p of input j
+__device__ __forceinline__ void transpose_bytes4x4(uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                                   uint32_t* out) {
+  const uint32_t t0 = __byte_perm(a, b, 0x5140);  // a0 b0 a1 b1
+  const uint32_t t1 = __byte_perm(c, d, 0x5140);  // c0 d0 c1 d1
+  const uint32_t t2 = __byte_perm(a, b, 0x7362);  // a2 b2 a3 b3
+  const uint32_t t3 = __byte_perm(c, d, 0x7362);  // c2 d2 c3 d3
+  out[0] = __byte_perm(t0, t1, 0x5410);           // a0 b0 c0 d0
+  out[1] = __byte_perm(t0, t1, 0x7632);           // a1 b1 c1 d1
+  out[2] = __byte_perm(t2, t3, 0x5410);           // a2 b2 c2 d2
+  out[3] = __byte_perm(t2, t3, 0x7632);           // a3 b3 c3 d3
+}
+
+// Writes 32 consecutive K entries of one tile row into the four planes
+// [plane][row][Kcap] (32 bytes per plane): x(i) returns the row's value at
+// K index k0 + i, f = split_row_factor(e) of the row.
+template <class F>
+__device__ __forceinline__ void write_row_digits32(F x, double f, int8_t* __restrict__ P, int row,
+                                                   int64_t Kcap, int k0) {
+  uint32_t pw[kSplitPlanes][8];
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) w[i] = pack_digits(rint_i32(x(4 * g + i) * f));
+    uint32_t pl[4];
+    transpose_bytes4x4(w[0], w[1], w[2], w[3], pl);
+#pragma unroll
+    for (int p = 0; p < kSplitPlanes; ++p) pw[p][g] = pl[p];
+  }
+#pragma unroll
+  for (int p = 0; p < kSplitPlanes; ++p) {
+    uint4* dst = reinterpret_cast<uint4*>(P + ((int64_t)p * kSplitRows + row) * Kcap + k0);
+    dst[0] = make_uint4(pw[p][0], pw[p][1], pw[p][2], pw[p][3]);
+    dst[1] = make_uint4(pw[p][4], pw[p][5], pw[p][6], pw[p][7]);
+  }
+}
+
+}  // namespace ctc

@@ -35,8 +35,12 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
+#include <cstdio>
+#include <cstdlib>
 
 #include "ctc_internal.h"
+#include "ctc_split.cuh"
 
 namespace ctc {
 
@@ -44,15 +48,16 @@ namespace {
 
 constexpr int kN = 64;          // nu columns per TMEM accumulator
 constexpr int kBK = 64;         // K bytes per pipeline stage
-constexpr int kStages = 4;
-constexpr int kRows = 128;      // tile rows (MMA M)
+constexpr int kStages = 3;
+constexpr int kRows = kSplitRows;  // tile rows (MMA M)
 constexpr int kLevels = 5;
-constexpr int kPlanes = 4;
+constexpr int kPlanes = kSplitPlanes;
 constexpr int kAPlaneBytes = kRows * kBK;       // 8 KB
 constexpr int kBPlaneBytes = kN * kBK;          // 4 KB
 constexpr int kAStageBytes = kPlanes * kAPlaneBytes;
 constexpr int kBStageBytes = kPlanes * kBPlaneBytes;
-constexpr int kSmemTc = kStages * (kAStageBytes + kBStageBytes) + 1024;  // + alignment slack
+constexpr int kGBytes = kN * kRows * 8;         // FP64 copy of one nu tile of G (64 KB)
+constexpr int kSmemTc = kStages * (kAStageBytes + kBStageBytes) + kGBytes + 1024;  // + alignment slack
 constexpr int kThreadsTc = 288;
 constexpr int kMaxKt = 16384;
 constexpr uint32_t kStatusTimeout = 0x7101;
@@ -105,13 +110,41 @@ __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1,
-                                            uint64_t* bar) {
+// L2 eviction policies: the tile's int8 A planes (re-read once per nu tile)
+// and the packed D (read by every tile) are kept; the FP64 AO values read once
+// by the epilogue are evicted first.
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* map, int c0, int c1,
+                                                 uint64_t* bar, uint64_t policy) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-          smem_u32(dst)),
-      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3}], [%4], %5;\n" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(smem_u32(bar)), "l"(policy)
       : "memory");
+}
+
+__device__ __forceinline__ uint32_t ldg_u32_hint(const uint32_t* p, uint64_t policy) {
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;\n" : "=r"(v) : "l"(p), "l"(policy));
+  return v;
+}
+
+__device__ __forceinline__ double ldg_f64_stream(const double* p, uint64_t policy) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;\n"
+               : "=d"(v)
+               : "l"(p), "l"(policy));
+  return v;
 }
 
 // K-major, 64-byte swizzle: 8-row atoms of 512 B, rows 64 B apart.
@@ -157,30 +190,105 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* v) {
 __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
+// Orders the use of tcgen05.ld results after tcgen05.wait::ld: the values pass
+// through an empty volatile asm placed after the wait.
+__device__ __forceinline__ void after_wait16(int32_t* v) {
+  asm volatile(""
+               : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]),
+                 "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]),
+                 "+r"(v[13]), "+r"(v[14]), "+r"(v[15]));
+}
 
-// balanced base-256 digits of |I| <= 2^30, most significant first, packed in a word
-__device__ __forceinline__ uint32_t pack_digits(int32_t I) {
-  uint32_t w = 0;
+// x 2^S exactly, for int32 x and 0 <= S <= 48, with one integer and one FP64
+// add (the exponent-bias construction of integer-to-double conversion): the
+// bit pattern (1075 + S) << 52 | (x + 2^31) is the double 2^(52+S) + (x + 2^31) 2^S,
+// and subtracting 2^(52+S) + 2^(31+S) leaves x 2^S.
+template <int S>
+__device__ __forceinline__ double i32_times_pow2(int32_t x) {
+  const long long hi = (long long)(1075 + S) << 52;
+  const double t = __longlong_as_double(hi | (long long)((uint32_t)x ^ 0x80000000u));
+  return t - __longlong_as_double(hi | (1ll << 31));
+}
+
+// Epilogue contraction roles for tiles of 32 points x {phi, d_x, d_y, d_z}
+// (NQA = 4).  Per point the epilogue needs 16 row sums
+//   s[q'] = sum_nu G0 A_q'        (q' = 0..9: phi, first and second derivatives)
+//   s[10..12] = sum_nu Gx A_{x,y,z},  s[13..14] = sum_nu Gy A_{y,z},  s[15] = sum_nu Gz A_z
+// where A_q' is the AO quantity q' at the point and G0..Gz the rows of G.  Each
+// of the four epilogue warps loads two or three AO quantities and forms the
+// sums that use them (4-5 dot products per point each):
+//   role 0: q' = 3 (rows 0,1,2,3 -> s3, s12, s14, s15), q' = 4 (s4)
+//   role 1: q' = 2 (rows 0,1,2 -> s2, s11, s13),        q' = 5 (s5)
+//   role 2: q' = 1 (rows 0,1 -> s1, s10), q' = 6 (s6), q' = 7 (s7)
+//   role 3: q' = 0 (s0), q' = 8 (s8), q' = 9 (s9)
+__device__ __forceinline__ constexpr int role_nslot(int role) { return role < 2 ? 2 : 3; }
+__device__ __forceinline__ constexpr int role_q(int role, int slot) {
+  return role == 0 ? (slot == 0 ? 3 : 4)
+       : role == 1 ? (slot == 0 ? 2 : 5)
+       : role == 2 ? (slot == 0 ? 1 : (slot == 1 ? 6 : 7))
+                   : (slot == 0 ? 0 : (slot == 1 ? 8 : 9));
+}
+// number of G rows (0, 1, ...) paired with the slot's quantity
+__device__ __forceinline__ constexpr int role_nrow(int role, int slot) {
+  return slot == 0 ? (role == 0 ? 4 : (role == 1 ? 3 : (role == 2 ? 2 : 1))) : 1;
+}
+// index into the 16 per-point sums of (slot, G row)
+__device__ __forceinline__ constexpr int role_sum(int role, int slot, int row) {
+  return row == 0 ? role_q(role, slot)
+       : role == 0 ? (row == 1 ? 12 : (row == 2 ? 14 : 15))
+       : role == 1 ? (row == 1 ? 11 : 13)
+                   : 10;
+}
+
+// One nu tile of the contraction for NQA = 4 and one role: acc[i] accumulates
+// the role's i-th sum (slot-major, rows in order).  G is the FP64 copy in
+// shared memory, [column][row]; ao points at AO quantity 0, column 0 of the nu
+// tile for this thread's point (element (q, c) at ao[q * ldq + c * 32]).
+template <int ROLE>
+__device__ __forceinline__ void contract_role(const double* __restrict__ ao, int64_t ldq,
+                                              const double* __restrict__ sG, int lane, int nq_ao,
+                                              uint64_t stream, double* acc) {
+  constexpr int NS = role_nslot(ROLE);
+  constexpr int NG = kN / 8;  // groups of 8 columns
+  bool live[NS];
 #pragma unroll
-  for (int p = 3; p >= 1; --p) {
-    const int32_t d = ((I + 128) & 255) - 128;
-    w |= (uint32_t)(d & 255) << (8 * p);
-    I = (I - d) >> 8;
+  for (int s = 0; s < NS; ++s) live[s] = role_q(ROLE, s) < nq_ao;
+  // two register buffers: the loads of group g + 1 are in flight while group g
+  // is reduced
+  double a[2][NS][8];
+  auto load = [&](int buf, int cg) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        a[buf][s][j] = live[s] ? ldg_f64_stream(ao + role_q(ROLE, s) * ldq + (cg + j) * 32, stream) : 0.0;
+  };
+  load(0, 0);
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    if (g + 1 < NG) load((g + 1) & 1, (g + 1) * 8);
+    const int cg = g * 8;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const double* gp = sG + (cg + j) * kRows + lane;
+      int i = 0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int rr = 0; rr < role_nrow(ROLE, s); ++rr, ++i)
+          acc[i] = fma(gp[rr * 32], a[g & 1][s][j], acc[i]);
+    }
   }
-  w |= (uint32_t)(I & 255);
-  return w;
 }
 
-__device__ __forceinline__ int32_t to_fixed(double x, int e) {
-  // |x| < 2^e  ->  |rint(x 2^(30-e))| <= 2^30
-  return (int32_t)llrint(ldexp(x, 30 - e));
-}
-
-__device__ __forceinline__ int scale_exponent(double amax) {
-  if (!(amax > 0.0)) return 0;
-  int e;
-  frexp(amax, &e);  // amax = m 2^e, m in [0.5, 1)
-  return e;
+template <int ROLE>
+__device__ __forceinline__ void store_role(double (*s_sums)[16], int lane, const double* acc) {
+  constexpr int NS = role_nslot(ROLE);
+  int i = 0;
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int rr = 0; rr < role_nrow(ROLE, s); ++rr, ++i) s_sums[lane][role_sum(ROLE, s, rr)] = acc[i];
 }
 
 // ------------------------------------------------------------------ preparation kernels
@@ -203,50 +311,9 @@ __global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint32_t*
   __syncthreads();
   const int e = scale_exponent(red[0]);
   if (threadIdx.x == 0) fexp[row] = e;
+  const double f = split_row_factor(e);
   for (int k = threadIdx.x; k < Mpad; k += blockDim.x)
-    Dp[(int64_t)row * Mpad + k] = pack_digits(to_fixed(d[k], e));
-}
-
-// Tile A rows (FP64, compact K, block layout [q][k][point]) -> four int8
-// planes [t][plane][row][Kcap] (row = q * PTS + point, K contiguous) and row
-// exponents.  Each lane owns one row: the row maximum reads consecutive points
-// across lanes, and every lane then writes 32 bytes per plane per step.
-__global__ void slice_a_kernel(TileBatch tb, int nqa, int8_t* __restrict__ planes,
-                               int32_t* __restrict__ eexp) {
-  const int t = blockIdx.x;
-  const int kt = tb.kt[t];
-  const int PTS = kRows / nqa;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t ldq = (int64_t)PTS * tb.Kcap;
-  const double* A = tb.ao + (int64_t)t * tb.nq * ldq;
-  int8_t* P = planes + (int64_t)t * kPlanes * kRows * tb.Kcap;
-  for (int r = warp * 32 + lane; r < kRows; r += blockDim.x) {
-    const int q = r / PTS, pl = r % PTS;
-    const double* col = A + q * ldq + pl;  // element k at col[k * PTS]
-    double m = 0.0;
-    for (int k = 0; k < kt; ++k) m = fmax(m, fabs(col[(int64_t)k * PTS]));
-    const int e = scale_exponent(m);
-    eexp[(int64_t)t * kRows + r] = e;
-    for (int k0 = 0; k0 < kt; k0 += 32) {
-      uint32_t pw[kPlanes][8];
-#pragma unroll
-      for (int g = 0; g < 8; ++g) {
-        uint32_t w[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = pack_digits(to_fixed(col[(int64_t)(k0 + 4 * g + i) * PTS], e));
-#pragma unroll
-        for (int p = 0; p < kPlanes; ++p)
-          pw[p][g] = ((w[0] >> (8 * p)) & 255) | (((w[1] >> (8 * p)) & 255) << 8) |
-                     (((w[2] >> (8 * p)) & 255) << 16) | (((w[3] >> (8 * p)) & 255) << 24);
-      }
-#pragma unroll
-      for (int p = 0; p < kPlanes; ++p) {
-        uint4* dst = reinterpret_cast<uint4*>(P + ((int64_t)p * kRows + r) * tb.Kcap + k0);
-        dst[0] = make_uint4(pw[p][0], pw[p][1], pw[p][2], pw[p][3]);
-        dst[1] = make_uint4(pw[p][4], pw[p][5], pw[p][6], pw[p][7]);
-      }
-    }
-  }
+    Dp[(int64_t)row * Mpad + k] = pack_digits(rint_i32(d[k] * f));
 }
 
 // ------------------------------------------------------------------ main kernel
@@ -260,6 +327,10 @@ struct TcArgs {
   ctc_outputs out;
   ctc_params prm;
   int32_t* status;
+  // optional per-tile cycle counters (CTC_TC_TRACE): [C][8] = total, producer
+  // wait on empty, producer stage work, MMA wait on full, MMA wait on tempty,
+  // epilogue wait on tfull, drain, contraction
+  long long* trace;
 };
 
 __device__ __forceinline__ void finalize_point_tc(const double* s, int nqa, int nq_ao,
@@ -274,12 +345,14 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   __shared__ __align__(8) uint64_t tfull_bar, tempty_bar, done_bar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int s_abort;
+  __shared__ int s_epi_abort[2];
   __shared__ double s_sums[32][16];
   __shared__ double s_cscale[2][kN];
 
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = smem;
   uint8_t* sB = smem + kStages * kAStageBytes;
+  double* sG = (double*)(smem + kStages * (kAStageBytes + kBStageBytes));  // [kN][kRows]
 
   const TileBatch& tb = args.tb;
   const int t = blockIdx.x;
@@ -308,57 +381,78 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
+  const long long t_start = clock64();
+  long long tr0 = 0, tr1 = 0, tr2 = 0;  // per-role trace counters
 
   if (warp < 4) {
     // ---------------- producers
     // Thread tid owns the 4 mu columns k4 = (tid % 16) * 4 of every stage and the
-    // 8 nu rows n = tid / 16 + 8 i of every nu tile, so its AO indices are
-    // loaded once per stage / tile and its 32 gathers of D are independent.
+    // 8 nu rows n = tid / 16 + 8 i of every nu tile; its 32 gathers of D are
+    // independent.  Stages are software-pipelined one ahead: the AO indices of
+    // stage it + 1 are requested before the wait for stage it's slot, and its
+    // gathers right after stage it's shared-memory writes, so the two
+    // dependent global latencies overlap the MMAs instead of adding up.
     const int tid = threadIdx.x;
     const int k4 = (tid & 15) * 4, nrow0 = tid >> 4;
-    int it = 0;
-    for (int nt = 0; nt < nnt && !s_abort; ++nt) {
-      const int n0 = nt * kN;
-      int nu[8];
+    const uint64_t keep = policy_evict_last();
+    const int nst = nnt * nkb;
+    auto load_idx = [&](int it, int (&nu)[8], int (&mu)[4]) {
+      const int nt = it / nkb, kb = it - nt * nkb;
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const int nc = n0 + nrow0 + 8 * i;
+        const int nc = nt * kN + nrow0 + 8 * i;
         nu[i] = nc < kt ? am[nc] : -1;
       }
-      for (int kb = 0; kb < nkb; ++kb, ++it) {
-        const int s = it % kStages;
-        const uint32_t ph = (it / kStages) & 1;
-        const int k0 = kb * kBK;
-        int mu[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) mu[j] = am[k0 + k4 + j];
-        uint32_t w[8][4];
+      for (int j = 0; j < 4; ++j) mu[j] = am[kb * kBK + k4 + j];
+    };
+    auto gather = [&](const int (&nu)[8], const int (&mu)[4], uint32_t (&w)[8][4]) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < 8; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
-            w[i][j] = (nu[i] >= 0 && mu[j] >= 0) ? __ldg(args.Dp + (int64_t)nu[i] * args.Mpad + mu[j]) : 0u;
-        if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
-        if (tid == 0) {
-          mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
-          for (int p = 0; p < kPlanes; ++p)
-            tma_load_2d(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0, (t * kPlanes + p) * kRows,
-                        &full_bar[s]);
-        }
-        uint8_t* b = sB + s * kBStageBytes;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const uint32_t off = sw64_offset(nrow0 + 8 * i, k4);
-#pragma unroll
-          for (int p = 0; p < kPlanes; ++p) {
-            const uint32_t v = ((w[i][0] >> (8 * p)) & 255) | (((w[i][1] >> (8 * p)) & 255) << 8) |
-                               (((w[i][2] >> (8 * p)) & 255) << 16) | (((w[i][3] >> (8 * p)) & 255) << 24);
-            *(uint32_t*)(b + p * kBPlaneBytes + off) = v;
-          }
-        }
-        fence_proxy_async();
-        mbar_arrive(&full_bar[s]);
+        for (int j = 0; j < 4; ++j)
+          w[i][j] = (nu[i] >= 0 && mu[j] >= 0)
+                        ? ldg_u32_hint(args.Dp + (int64_t)nu[i] * args.Mpad + mu[j], keep)
+                        : 0u;
+    };
+    int nu[8], mu[4];
+    uint32_t w[8][4];
+    if (nst > 0) {
+      load_idx(0, nu, mu);
+      gather(nu, mu, w);
+    }
+    for (int it = 0; it < nst && !s_abort; ++it) {
+      const bool more = it + 1 < nst;
+      if (more) load_idx(it + 1, nu, mu);
+      const int s = it % kStages;
+      const uint32_t ph = (it / kStages) & 1;
+      const int k0 = (it % nkb) * kBK;
+      const long long tw = clock64();
+      if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
+      tr0 += clock64() - tw;
+      if (tid == 0) {
+        mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
+        for (int p = 0; p < kPlanes; ++p)
+          tma_load_2d_hint(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0,
+                           (t * kPlanes + p) * kRows, &full_bar[s], keep);
       }
+      uint8_t* b = sB + s * kBStageBytes;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        // 4 words of 4 digit bytes -> 4 plane words of 4 consecutive mu
+        uint32_t pl[4];
+        transpose_bytes4x4(w[i][0], w[i][1], w[i][2], w[i][3], pl);
+        const uint32_t off = sw64_offset(nrow0 + 8 * i, k4);
+#pragma unroll
+        for (int p = 0; p < kPlanes; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
+      }
+      fence_proxy_async();
+      mbar_arrive(&full_bar[s]);
+      if (more) gather(nu, mu, w);
+    }
+    if (args.trace && tid == 0) {
+      args.trace[(int64_t)t * 8 + 1] = tr0;
+      args.trace[(int64_t)t * 8 + 2] = clock64() - t_start - tr0;
     }
   } else if (warp == 4) {
     // ---------------- MMA issuer
@@ -366,13 +460,17 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
                            ((uint32_t)(kRows >> 4) << 24);
     int it = 0;
     for (int nt = 0; nt < nnt && !s_abort; ++nt) {
+      const long long tw = clock64();
       if (!mbar_wait(&tempty_bar, (nt & 1) ^ 1)) { s_abort = 1; break; }
+      tr1 += clock64() - tw;
       tc_fence_after();
       uint32_t started = 0;  // bit L: level L accumulator initialised
       for (int kb = 0; kb < nkb; ++kb, ++it) {
         const int s = it % kStages;
         const uint32_t ph = (it / kStages) & 1;
+        const long long tf = clock64();
         if (!mbar_wait(&full_bar[s], ph)) { s_abort = 1; break; }
+        tr0 += clock64() - tf;
         tc_fence_after();
         if (lane == 0) {
           const uint32_t a0 = smem_u32(sA + s * kAStageBytes);
@@ -401,24 +499,33 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       if (lane == 0) umma_commit(&tfull_bar);
       __syncwarp();
     }
+    if (args.trace && lane == 0) {
+      args.trace[(int64_t)t * 8 + 3] = tr0;
+      args.trace[(int64_t)t * 8 + 4] = tr1;
+    }
   } else {
     // ---------------- epilogue (warps 5..8 -> TMEM lane quarters 1,2,3,0)
+    // Per nu tile: drain the five level accumulators of this warp's TMEM lane
+    // quarter into one FP64 value per element, scaled, in the shared-memory
+    // copy of G; release TMEM (the MMA warp starts the next nu tile); then
+    // contract G with the FP64 AO values while those MMAs run.
     const int quarter = warp & 3;
-    const int r = quarter * 32 + lane;
-    const int etid = (warp - 5) * 32 + lane;  // 0..127
+    const int r = quarter * 32 + lane;        // TMEM lane / G row drained by this thread
+    const int role = warp - 5;                // 0..3
+    const int etid = role * 32 + lane;        // 0..127
     constexpr int PTS = kRows / NQA;
-    const int q = r / PTS, pl = r % PTS;
     const int nq_ao = tb.nq;
     const int64_t ldq = (int64_t)tb.TP * tb.Kcap;
-    const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pl;  // element (q, k) at aop[q*ldq + k*PTS]
-    const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 60);
-    // quantities this row is reduced against: q = 0 -> phi, d phi, d2 phi; q = k -> d_j phi, j >= k
-    const int qa = (q == 0) ? 0 : q;
-    const int qb = (q == 0) ? nq_ao : 4;
-    double sums[10];
-#pragma unroll
-    for (int i = 0; i < 10; ++i) sums[i] = 0.0;
-    for (int nt = 0; nt < nnt && !s_abort; ++nt) {
+    // point contracted by this thread: NQA = 4 -> lane (all roles share the 32
+    // points, each with its own AO quantities); NQA = 1 -> the role's 32 rows
+    const int pc = (NQA == 4) ? lane : etid;
+    const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pc;  // element (q, k) at aop[q*ldq + k*PTS]
+    // G = 2^(e_r + f_nu - 60) sum_L acc_L 2^(48 - 8 L); the drain below forms
+    // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^16
+    const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 44);
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const uint64_t stream = policy_evict_first();
+    for (int nt = 0; nt < nnt; ++nt) {
       const int n0 = nt * kN;
       double* cs = s_cscale[nt & 1];
       if (etid < kN) {
@@ -426,65 +533,97 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         const int nu = nc < kt ? am[nc] : -1;
         cs[etid] = nu >= 0 ? ldexp(1.0, args.fexp[nu]) : 0.0;
       }
+      // (A) column scales written; every role has finished reading sG
       asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      if (!mbar_wait(&tfull_bar, nt & 1)) { s_abort = 1; break; }
+      // uniform stop decision: the flag slot read here was written before (B)
+      // of the previous nu tile
+      if (nt > 0 && s_epi_abort[(nt - 1) & 1]) break;
+      const long long te = clock64();
+      if (!mbar_wait(&tfull_bar, nt & 1)) s_abort = 1;
+      const long long td = clock64();
+      tr0 += td - te;
       tc_fence_after();
 #pragma unroll 1
       for (int c = 0; c < kN / 16; ++c) {
-        double g[16];
+        int32_t v[kLevels][16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) g[j] = 0.0;
+        for (int L = 0; L < kLevels; ++L)
+          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + L * kN + c * 16, v[L]);
+        tmem_ld_wait();
 #pragma unroll
-        for (int L = 0; L < kLevels; ++L) {
-          int32_t v[16];
-          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + L * kN + c * 16, v);
-          tmem_ld_wait();
-          const double w = ldexp(1.0, 48 - 8 * L);
+        for (int L = 0; L < kLevels; ++L) after_wait16(v[L]);
 #pragma unroll
-          for (int j = 0; j < 16; ++j) g[j] += (double)v[j] * w;
-        }
-#pragma unroll
-        for (int j = 0; j < 16; ++j) g[j] *= rowscale * cs[c * 16 + j];
-        const int col = n0 + c * 16;
-        for (int qq = qa; qq < qb; ++qq) {
-          const double* src = aop + qq * ldq + (int64_t)col * PTS;
-          double v[16];
-#pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = __ldg(src + j * PTS);
-          double acc = 0.0;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) acc += g[j] * v[j];
-          sums[qq - qa] += acc;
+        for (int j = 0; j < 16; ++j) {
+          // sum_L acc_L 2^(48 - 8 L), smallest terms first
+          double g = i32_times_pow2<0>(v[4][j]);
+          g += i32_times_pow2<8>(v[3][j]);
+          g += i32_times_pow2<16>(v[2][j]);
+          g += i32_times_pow2<24>(v[1][j]);
+          g += i32_times_pow2<32>(v[0][j]);
+          sG[(c * 16 + j) * kRows + r] = g * rowscale * cs[c * 16 + j];
         }
       }
       tc_fence_before();
       mbar_arrive(&tempty_bar);
-    }
-    // gather the per-row sums of each point and finalise
-    asm volatile("bar.sync 1, 128;\n" ::: "memory");
-    if (NQA == 4) {
-      if (q == 0) {
-        for (int i = 0; i < 10; ++i) s_sums[pl][i] = sums[i];
-      } else if (q == 1) {
-        s_sums[pl][10] = sums[0]; s_sums[pl][11] = sums[1]; s_sums[pl][12] = sums[2];
-      } else if (q == 2) {
-        s_sums[pl][13] = sums[0]; s_sums[pl][14] = sums[1];
+      const long long tc0 = clock64();
+      tr1 += tc0 - td;
+      if (etid == 0) s_epi_abort[nt & 1] = s_abort;
+      // (B) G of this nu tile complete in shared memory
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      const double* ao_nt = aop + (int64_t)n0 * PTS;
+      if (NQA == 4) {
+        switch (role) {
+          case 0: contract_role<0>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+          case 1: contract_role<1>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+          case 2: contract_role<2>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+          default: contract_role<3>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+        }
       } else {
-        s_sums[pl][15] = sums[0];
+        // rows are points: sums over the nq_ao (1 or 4) quantities of this point
+#pragma unroll 4
+        for (int c = 0; c < kN; ++c) {
+          const double g = sG[c * kRows + etid];
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq)
+            if (qq < nq_ao) acc[qq] = fma(g, ldg_f64_stream(ao_nt + qq * ldq + c * PTS, stream), acc[qq]);
+        }
+      }
+      if (args.trace) {
+        // results of the contraction are complete when they are used
+        double chk = acc[0] + acc[1] + acc[2] + acc[3] + acc[4];
+        asm volatile("" : "+d"(chk));
+        tr2 += clock64() - tc0;
+      }
+    }
+    if (args.trace && etid == 0) {
+      args.trace[(int64_t)t * 8 + 5] = tr0;
+      args.trace[(int64_t)t * 8 + 6] = tr1;
+      args.trace[(int64_t)t * 8 + 7] = tr2;
+    }
+    // (C) gather the per-point sums and finalise
+    asm volatile("bar.sync 1, 128;\n" ::: "memory");
+    const bool aborted = s_abort != 0;
+    if (NQA == 4) {
+      switch (role) {
+        case 0: store_role<0>(s_sums, lane, acc); break;
+        case 1: store_role<1>(s_sums, lane, acc); break;
+        case 2: store_role<2>(s_sums, lane, acc); break;
+        default: store_role<3>(s_sums, lane, acc); break;
       }
       asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      if (q == 0 && !s_abort) {
-        const int64_t oidx = tb.out[(int64_t)t * tb.TP + pl];
-        if (oidx >= 0) finalize_point_tc(s_sums[pl], 4, nq_ao, args.out, oidx, args.prm);
+      if (role == 0 && !aborted) {
+        const int64_t oidx = tb.out[(int64_t)t * tb.TP + lane];
+        if (oidx >= 0) finalize_point_tc(s_sums[lane], 4, nq_ao, args.out, oidx, args.prm);
       }
-    } else if (!s_abort) {
-      const int64_t oidx = tb.out[(int64_t)t * tb.TP + pl];
+    } else if (!aborted) {
+      const int64_t oidx = tb.out[(int64_t)t * tb.TP + etid];
       double s16[16];
-      for (int i = 0; i < 16; ++i) s16[i] = i < 4 ? sums[i] : 0.0;
+      for (int i = 0; i < 16; ++i) s16[i] = i < 4 ? acc[i] : 0.0;
       if (oidx >= 0) finalize_point_tc(s16, 1, nq_ao, args.out, oidx, args.prm);
     }
   }
   __syncthreads();
+  if (args.trace && threadIdx.x == 0) args.trace[(int64_t)t * 8] = clock64() - t_start;
   if (s_abort && threadIdx.x == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
   if (warp == 4) {
     // every MMA this thread issued has completed before TMEM is released
@@ -571,6 +710,17 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
   return CTC_OK;
 }
 
+int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
+                       int32_t** eexp) {
+  const size_t plane_bytes = (size_t)tb.C * kPlanes * kRows * tb.Kcap;
+  const size_t need = plane_bytes + 256 + sizeof(int32_t) * (size_t)tb.C * kRows;
+  int rc = mol->ws_sl.ensure(need, st);
+  if (rc != CTC_OK) return rc;
+  *planes = (int8_t*)mol->ws_sl.p;
+  *eexp = (int32_t*)((char*)mol->ws_sl.p + (plane_bytes + 255) / 256 * 256);
+  return CTC_OK;
+}
+
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
@@ -578,14 +728,11 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
     return fail(CTC_ERR_UNSUPPORTED, "tensor-core split path: more than 16384 functions per tile");
   int rc = prepare_tc(mol, st);
   if (rc != CTC_OK) return rc;
-  // int8 planes of the tile rows + row exponents
-  const size_t plane_bytes = (size_t)tb.C * kPlanes * kRows * tb.Kcap;
-  const size_t need = plane_bytes + 256 + sizeof(int32_t) * (size_t)tb.C * kRows;
-  if ((rc = mol->ws_sl.ensure(need, st)) != CTC_OK) return rc;
-  int8_t* planes = (int8_t*)mol->ws_sl.p;
-  int32_t* eexp = (int32_t*)((char*)mol->ws_sl.p + (plane_bytes + 255) / 256 * 256);
-  slice_a_kernel<<<tb.C, 256, 0, st>>>(tb, plan.nqa, planes, eexp);
-  CTC_CUDA_TRY(cudaGetLastError());
+  // int8 planes of the tile rows + row exponents, written by this chunk's AO
+  // kernel (launch_ao_tiles_sliced)
+  int8_t* planes = nullptr;
+  int32_t* eexp = nullptr;
+  if ((rc = tc_slice_workspace(mol, tb, st, &planes, &eexp)) != CTC_OK) return rc;
   // tensor map over the planes: 2-D, rows = C*4*128, inner = Kcap bytes
   PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode();
   if (!enc) return fail(CTC_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
@@ -608,6 +755,11 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   a.out = *out;
   a.prm = *prm;
   a.status = mol->d_status;
+  a.trace = nullptr;
+  // CTC_TC_TRACE=1: per-tile cycle counters of the kernel's roles, summarised
+  // on stderr after each launch (synchronises the stream; diagnostics only)
+  static const bool trace_on = std::getenv("CTC_TC_TRACE") != nullptr;
+  if (trace_on) CTC_CUDA_TRY(cudaMallocAsync((void**)&a.trace, sizeof(long long) * 8 * tb.C, st));
   static bool attr[2] = {false, false};
   ProfScope ps(mol, 0, st);
   if (plan.nqa == 4) {
@@ -624,6 +776,28 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
     tc_tile_kernel<1><<<tb.C, kThreadsTc, kSmemTc, st>>>(amap, a);
   }
   CTC_CUDA_TRY(cudaGetLastError());
+  if (trace_on) {
+    std::vector<long long> tr((size_t)8 * tb.C);
+    std::vector<int32_t> kt(tb.C);
+    CTC_CUDA_TRY(cudaMemcpyAsync(tr.data(), a.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost, st));
+    CTC_CUDA_TRY(cudaMemcpyAsync(kt.data(), tb.kt, sizeof(int32_t) * tb.C, cudaMemcpyDeviceToHost, st));
+    CTC_CUDA_TRY(cudaStreamSynchronize(st));
+    CTC_CUDA_TRY(cudaFreeAsync(a.trace, st));
+    double sum[8] = {0}, stages = 0, ktmax = 0, ktsum = 0;
+    for (int i = 0; i < tb.C; ++i) {
+      for (int k = 0; k < 8; ++k) sum[k] += (double)tr[(size_t)8 * i + k];
+      const double nk = kt[i] / (double)kBK;
+      stages += nk * nk;
+      ktsum += kt[i];
+      ktmax = std::max(ktmax, (double)kt[i]);
+    }
+    std::fprintf(stderr,
+                 "[ctc tc trace] tiles %d mean kt %.0f max kt %.0f | cycles per stage: total %.0f "
+                 "prod_wait_empty %.0f prod_work %.0f mma_wait_full %.0f mma_wait_tempty %.0f "
+                 "epi_wait_tfull %.0f epi_drain %.0f epi_contract %.0f\n",
+                 tb.C, ktsum / tb.C, ktmax, sum[0] / stages, sum[1] / stages, sum[2] / stages,
+                 sum[3] / stages, sum[4] / stages, sum[5] / stages, sum[6] / stages, sum[7] / stages);
+  }
   return CTC_OK;
 }
 

@@ -530,9 +530,11 @@ size_t tile_bytes(const ctc_molecule* mol, int C, int TP) {
 
 
 // Tile builder + chunk loop.  For every chunk: tile points, screen, AO block
-// (derivative order deriv, nq quantities), then compute(tb).
+// (derivative order deriv, nq quantities; ao_launch replaces the plain AO
+// kernel launch when given), then compute(tb).
 inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, int nq, int deriv,
-                     cudaStream_t st, const std::function<int(const TileBatch&)>& compute) {
+                     cudaStream_t st, const std::function<int(const TileBatch&)>& compute,
+                     const std::function<int(const TileBatch&)>* ao_launch = nullptr) {
   int TX = 2, TY = 4, TZ = 4;
   if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
   int64_t ntiles, nbx = 0, nby = 0, nbz = 0;
@@ -623,7 +625,8 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     CTC_CUDA_TRY(cudaGetLastError());
     {
       ProfScope ps(mol, 1, st);
-      if ((rc = launch_ao_tiles(mol, tb, deriv, st)) != CTC_OK) return rc;
+      rc = ao_launch ? (*ao_launch)(tb) : launch_ao_tiles(mol, tb, deriv, st);
+      if (rc != CTC_OK) return rc;
     }
     mol->host_launches += 3;
     mol->host_chunks += 1;

@@ -57,6 +57,19 @@ def test_tc_density_only_variant(torch_cuda, case):
     _check(mol, pts, keys=("rho", "grad"))
 
 
+@pytest.mark.parametrize("case", ["allshell", "mixed"])
+def test_tc_first_derivative_rows_variant(torch_cuda, case):
+    """tau_PD without second-derivative outputs: 32-point tiles of phi and
+    grad phi rows over an AO block of value and first derivatives only."""
+    mol, pts = _cases().CASES[case]()
+    _check(mol, pts, keys=("rho", "grad", "tau_pd"))
+
+
+def test_tc_density_only_rows(torch_cuda):
+    mol, pts = _cases().CASES["allshell"]()
+    _check(mol, pts, keys=("rho",))
+
+
 def test_tc_large_molecule_slice(torch_cuda):
     """60 atoms of the 200-atom generator (pure d and f), cube points."""
     mol = S.make_molecule("c2", seed=4, natom=60, box=14.0, nocc=120)
