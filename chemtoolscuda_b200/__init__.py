@@ -3,7 +3,7 @@
 ``chemtools_cuda`` is the pybind11 module with the reference's ``Molecule``
 API; the sm_100a kernels behind it live in ``libchemtools_cuda.so`` (C ABI in
 ``include/chemtools_cuda.h``).  Importing fails loudly when the native library
-has not been built (``python -m chemtoolscuda_b200.build``): there is no CPU
+has not been built (``python chemtoolscuda_b200/build.py``): there is no CPU
 fallback.
 """
 from __future__ import annotations
@@ -17,7 +17,7 @@ try:
     from . import _chemtools_cuda as chemtools_cuda  # noqa: F401
 except ImportError as e:  # pragma: no cover - exercised only without a build
     raise ImportError(
-        "chemtoolscuda_b200: native extension not built; run `python -m chemtoolscuda_b200.build` "
+        "chemtoolscuda_b200: native extension not built; run `python chemtoolscuda_b200/build.py` "
         f"({e})") from e
 
 Molecule = chemtools_cuda.Molecule

@@ -1,7 +1,7 @@
 """Build the sm_100a library and its Python module in-tree.
 
-    python -m chemtoolscuda_b200.build          # incremental
-    python -m chemtoolscuda_b200.build --clean
+    python chemtoolscuda_b200/build.py          # incremental
+    python chemtoolscuda_b200/build.py --clean
 
 Produces
   chemtoolscuda_b200/libchemtools_cuda.so          the C ABI (include/chemtools_cuda.h)
