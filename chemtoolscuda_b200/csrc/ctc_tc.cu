@@ -20,14 +20,17 @@
 //     the FP64 path).
 // The dropped products (i + j >= 5) are below 2^-40 of the row/column scale.
 //
-// Kernel roles (288 threads): warps 0-3 produce the operands of each K block
-// (one thread issues the TMA loads of the four A planes; all 128 threads
-// gather the four D planes by compact index from the packed copy of D and
-// write them in the 64-byte-swizzled K-major layout), warp 4 issues the MMAs
-// from one thread and commits them to mbarriers, warps 5-8 read the TMEM
-// accumulators (one 32-lane quarter each) and run the FP64 epilogue.  Every
-// mbarrier wait is bounded: on timeout the kernel records a status code,
-// stops issuing work, and the allocating warp still frees its TMEM.
+// Kernel roles (288 threads, one persistent CTA per SM taking the chunk's
+// tiles largest first from a launch-wide counter): warps 0-3 produce the
+// operands of each K block (one thread issues the TMA loads of the four A
+// planes; all 128 threads gather the four D planes by compact index from the
+// packed copy of D and write them in the 64-byte-swizzled K-major layout),
+// warp 4 issues the MMAs from one thread and commits them to mbarriers, warps
+// 5-8 drain the TMEM accumulators (one 32-lane quarter each) into an FP64 copy
+// of G in shared memory and run the epilogue while the next nu tile's MMAs
+// run.  Every mbarrier wait is bounded: on timeout the kernel records a
+// status code, stops issuing work, and the allocating warp still frees its
+// TMEM.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -38,6 +41,8 @@
 #include <vector>
 #include <cstdio>
 #include <cstdlib>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "ctc_internal.h"
 #include "ctc_split.cuh"
@@ -61,6 +66,8 @@ constexpr int kSmemTc = kStages * (kAStageBytes + kBStageBytes) + kGBytes + 1024
 constexpr int kThreadsTc = 288;
 constexpr int kMaxKt = 16384;
 constexpr uint32_t kStatusTimeout = 0x7101;
+// readers of a tile-ring slot: 4 producer warps, the MMA warp, one epilogue thread
+constexpr uint32_t kTileReaders = 6;
 
 // ------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -327,9 +334,13 @@ struct TcArgs {
   ctc_outputs out;
   ctc_params prm;
   int32_t* status;
-  // optional per-tile cycle counters (CTC_TC_TRACE): [C][8] = total, producer
-  // wait on empty, producer stage work, MMA wait on full, MMA wait on tempty,
-  // epilogue wait on tfull, drain, contraction
+  // tile schedule: order[0..C) lists the chunk's tiles (largest compact K
+  // first); tile_counter (zero at launch) hands them out to the CTAs
+  const int32_t* order;
+  int32_t* tile_counter;
+  // optional per-CTA cycle counters (CTC_TC_TRACE): [grid][8] = total,
+  // producer wait on empty, producer stage work, MMA wait on full, MMA wait
+  // on tempty, epilogue wait on tfull, drain, contraction
   long long* trace;
 };
 
@@ -343,8 +354,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
   __shared__ __align__(8) uint64_t tfull_bar, tempty_bar, done_bar;
+  __shared__ __align__(8) uint64_t tile_full_bar[2], tile_empty_bar[2];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int s_abort;
+  __shared__ int s_tile[2];
+  __shared__ int s_epi_tile;
   __shared__ int s_epi_abort[2];
   __shared__ double s_sums[32][16];
   __shared__ double s_cscale[2][kN];
@@ -355,12 +369,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   double* sG = (double*)(smem + kStages * (kAStageBytes + kBStageBytes));  // [kN][kRows]
 
   const TileBatch& tb = args.tb;
-  const int t = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int kt = tb.kt[t];
-  const int nkb = kt / kBK;
-  const int nnt = (kt + kN - 1) / kN;
-  const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -370,6 +379,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     mbar_init(&tfull_bar, 1);
     mbar_init(&tempty_bar, 128);
     mbar_init(&done_bar, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&tile_full_bar[i], 1);
+      mbar_init(&tile_empty_bar[i], kTileReaders);
+    }
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -384,131 +397,182 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   const long long t_start = clock64();
   long long tr0 = 0, tr1 = 0, tr2 = 0;  // per-role trace counters
 
+  // The CTA's i-th tile arrives through slot i & 1 of a two-entry ring: the
+  // first producer thread takes the next index of the chunk's tile order from
+  // the launch-wide counter, publishes it (-1 when the chunk is exhausted) and
+  // every role reads it; a slot is refilled once all kTileReaders readers have
+  // released it.  Each role walks the same tile sequence at its own pace.
+  auto read_tile = [&](int i) -> int {
+    const int slot = i & 1;
+    int t = -1;
+    if (!mbar_wait(&tile_full_bar[slot], (i >> 1) & 1)) {
+      s_abort = 1;
+    } else {
+      t = s_tile[slot];
+    }
+    return t;
+  };
+
   if (warp < 4) {
     // ---------------- producers
     // Thread tid owns the 4 mu columns k4 = (tid % 16) * 4 of every stage and the
     // 8 nu rows n = tid / 16 + 8 i of every nu tile; its 32 gathers of D are
     // independent.  Stages are software-pipelined one ahead: the AO indices of
-    // stage it + 1 are requested before the wait for stage it's slot, and its
-    // gathers right after stage it's shared-memory writes, so the two
-    // dependent global latencies overlap the MMAs instead of adding up.
+    // stage j + 1 are requested before the wait for stage j's slot, and its
+    // gathers right after stage j's shared-memory writes, so the two dependent
+    // global latencies overlap the MMAs instead of adding up.
     const int tid = threadIdx.x;
     const int k4 = (tid & 15) * 4, nrow0 = tid >> 4;
     const uint64_t keep = policy_evict_last();
-    const int nst = nnt * nkb;
-    auto load_idx = [&](int it, int (&nu)[8], int (&mu)[4]) {
-      const int nt = it / nkb, kb = it - nt * nkb;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int nc = nt * kN + nrow0 + 8 * i;
-        nu[i] = nc < kt ? am[nc] : -1;
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) mu[j] = am[kb * kBK + k4 + j];
-    };
-    auto gather = [&](const int (&nu)[8], const int (&mu)[4], uint32_t (&w)[8][4]) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          w[i][j] = (nu[i] >= 0 && mu[j] >= 0)
-                        ? ldg_u32_hint(args.Dp + (int64_t)nu[i] * args.Mpad + mu[j], keep)
-                        : 0u;
-    };
-    int nu[8], mu[4];
-    uint32_t w[8][4];
-    if (nst > 0) {
-      load_idx(0, nu, mu);
-      gather(nu, mu, w);
-    }
-    for (int it = 0; it < nst && !s_abort; ++it) {
-      const bool more = it + 1 < nst;
-      if (more) load_idx(it + 1, nu, mu);
-      const int s = it % kStages;
-      const uint32_t ph = (it / kStages) & 1;
-      const int k0 = (it % nkb) * kBK;
-      const long long tw = clock64();
-      if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
-      tr0 += clock64() - tw;
+    int it = 0;  // stage counter across tiles
+    for (int i = 0;; ++i) {
       if (tid == 0) {
-        mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
-        for (int p = 0; p < kPlanes; ++p)
-          tma_load_2d_hint(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0,
-                           (t * kPlanes + p) * kRows, &full_bar[s], keep);
+        const int slot = i & 1;
+        int next = -1;
+        if (!mbar_wait(&tile_empty_bar[slot], ((i >> 1) & 1) ^ 1)) {
+          s_abort = 1;
+        } else {
+          const int c = atomicAdd(args.tile_counter, 1);
+          next = c < tb.C ? args.order[c] : -1;
+        }
+        s_tile[slot] = next;
+        mbar_arrive(&tile_full_bar[slot]);
       }
-      uint8_t* b = sB + s * kBStageBytes;
+      const int t = read_tile(i);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
+      if (t < 0 || s_abort) break;
+      const int kt = tb.kt[t];
+      const int nkb = kt / kBK;
+      const int nnt = (kt + kN - 1) / kN;
+      const int nst = nnt * nkb;
+      const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+      auto load_idx = [&](int j, int (&nu)[8], int (&mu)[4]) {
+        const int nt = j / nkb, kb = j - nt * nkb;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        // 4 words of 4 digit bytes -> 4 plane words of 4 consecutive mu
-        uint32_t pl[4];
-        transpose_bytes4x4(w[i][0], w[i][1], w[i][2], w[i][3], pl);
-        const uint32_t off = sw64_offset(nrow0 + 8 * i, k4);
+        for (int q = 0; q < 8; ++q) {
+          const int nc = nt * kN + nrow0 + 8 * q;
+          nu[q] = nc < kt ? am[nc] : -1;
+        }
 #pragma unroll
-        for (int p = 0; p < kPlanes; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
+        for (int q = 0; q < 4; ++q) mu[q] = am[kb * kBK + k4 + q];
+      };
+      auto gather = [&](const int (&nu)[8], const int (&mu)[4], uint32_t (&w)[8][4]) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+#pragma unroll
+          for (int m = 0; m < 4; ++m)
+            w[q][m] = (nu[q] >= 0 && mu[m] >= 0)
+                          ? ldg_u32_hint(args.Dp + (int64_t)nu[q] * args.Mpad + mu[m], keep)
+                          : 0u;
+      };
+      int nu[8], mu[4];
+      uint32_t w[8][4];
+      if (nst > 0) {
+        load_idx(0, nu, mu);
+        gather(nu, mu, w);
       }
-      fence_proxy_async();
-      mbar_arrive(&full_bar[s]);
-      if (more) gather(nu, mu, w);
+      for (int j = 0; j < nst; ++j, ++it) {
+        const bool more = j + 1 < nst;
+        if (more) load_idx(j + 1, nu, mu);
+        const int s = it % kStages;
+        const uint32_t ph = (it / kStages) & 1;
+        const int k0 = (j % nkb) * kBK;
+        const long long tw = clock64();
+        if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
+        tr0 += clock64() - tw;
+        if (tid == 0) {
+          mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
+          for (int p = 0; p < kPlanes; ++p)
+            tma_load_2d_hint(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0,
+                             (t * kPlanes + p) * kRows, &full_bar[s], keep);
+        }
+        uint8_t* b = sB + s * kBStageBytes;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          // 4 words of 4 digit bytes -> 4 plane words of 4 consecutive mu
+          uint32_t pl[4];
+          transpose_bytes4x4(w[q][0], w[q][1], w[q][2], w[q][3], pl);
+          const uint32_t off = sw64_offset(nrow0 + 8 * q, k4);
+#pragma unroll
+          for (int p = 0; p < kPlanes; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
+        }
+        fence_proxy_async();
+        mbar_arrive(&full_bar[s]);
+        if (more) gather(nu, mu, w);
+      }
+      if (s_abort) break;
     }
     if (args.trace && tid == 0) {
-      args.trace[(int64_t)t * 8 + 1] = tr0;
-      args.trace[(int64_t)t * 8 + 2] = clock64() - t_start - tr0;
+      args.trace[(int64_t)blockIdx.x * 8 + 1] = tr0;
+      args.trace[(int64_t)blockIdx.x * 8 + 2] = clock64() - t_start - tr0;
     }
   } else if (warp == 4) {
     // ---------------- MMA issuer
     const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
                            ((uint32_t)(kRows >> 4) << 24);
-    int it = 0;
-    for (int nt = 0; nt < nnt && !s_abort; ++nt) {
-      const long long tw = clock64();
-      if (!mbar_wait(&tempty_bar, (nt & 1) ^ 1)) { s_abort = 1; break; }
-      tr1 += clock64() - tw;
-      tc_fence_after();
-      uint32_t started = 0;  // bit L: level L accumulator initialised
-      for (int kb = 0; kb < nkb; ++kb, ++it) {
-        const int s = it % kStages;
-        const uint32_t ph = (it / kStages) & 1;
-        const long long tf = clock64();
-        if (!mbar_wait(&full_bar[s], ph)) { s_abort = 1; break; }
-        tr0 += clock64() - tf;
+    int it = 0, gnt = 0;  // stage and nu-tile counters across tiles
+    for (int i = 0;; ++i) {
+      const int t = read_tile(i);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
+      if (t < 0 || s_abort) break;
+      const int kt = tb.kt[t];
+      const int nkb = kt / kBK;
+      const int nnt = (kt + kN - 1) / kN;
+      for (int nt = 0; nt < nnt && !s_abort; ++nt, ++gnt) {
+        const long long tw = clock64();
+        if (!mbar_wait(&tempty_bar, (gnt & 1) ^ 1)) { s_abort = 1; break; }
+        tr1 += clock64() - tw;
         tc_fence_after();
-        if (lane == 0) {
-          const uint32_t a0 = smem_u32(sA + s * kAStageBytes);
-          const uint32_t b0 = smem_u32(sB + s * kBStageBytes);
+        uint32_t started = 0;  // bit L: level L accumulator initialised
+        for (int kb = 0; kb < nkb; ++kb, ++it) {
+          const int s = it % kStages;
+          const uint32_t ph = (it / kStages) & 1;
+          const long long tf = clock64();
+          if (!mbar_wait(&full_bar[s], ph)) { s_abort = 1; break; }
+          tr0 += clock64() - tf;
+          tc_fence_after();
+          if (lane == 0) {
+            const uint32_t a0 = smem_u32(sA + s * kAStageBytes);
+            const uint32_t b0 = smem_u32(sB + s * kBStageBytes);
 #pragma unroll
-          for (int ks = 0; ks < kBK / 32; ++ks) {
+            for (int ks = 0; ks < kBK / 32; ++ks) {
 #pragma unroll
-            for (int i = 0; i < kPlanes; ++i) {
+              for (int pa = 0; pa < kPlanes; ++pa) {
 #pragma unroll
-              for (int j = 0; j < kPlanes; ++j) {
-                const int L = i + j;
-                if (L >= kLevels) continue;
-                const uint64_t ad = umma_desc_sw64(a0 + i * kAPlaneBytes + ks * 32);
-                const uint64_t bd = umma_desc_sw64(b0 + j * kBPlaneBytes + ks * 32);
-                const uint32_t acc = (started >> L) & 1u;
-                umma_i8(tmem + L * kN, ad, bd, idesc, acc);
-                started |= 1u << L;
+                for (int pb = 0; pb < kPlanes; ++pb) {
+                  const int L = pa + pb;
+                  if (L >= kLevels) continue;
+                  const uint64_t ad = umma_desc_sw64(a0 + pa * kAPlaneBytes + ks * 32);
+                  const uint64_t bd = umma_desc_sw64(b0 + pb * kBPlaneBytes + ks * 32);
+                  const uint32_t acc = (started >> L) & 1u;
+                  umma_i8(tmem + L * kN, ad, bd, idesc, acc);
+                  started |= 1u << L;
+                }
               }
             }
+            umma_commit(&empty_bar[s]);
           }
-          umma_commit(&empty_bar[s]);
+          __syncwarp();
         }
+        if (s_abort) break;
+        if (lane == 0) umma_commit(&tfull_bar);
         __syncwarp();
       }
       if (s_abort) break;
-      if (lane == 0) umma_commit(&tfull_bar);
-      __syncwarp();
     }
     if (args.trace && lane == 0) {
-      args.trace[(int64_t)t * 8 + 3] = tr0;
-      args.trace[(int64_t)t * 8 + 4] = tr1;
+      args.trace[(int64_t)blockIdx.x * 8 + 3] = tr0;
+      args.trace[(int64_t)blockIdx.x * 8 + 4] = tr1;
     }
   } else {
     // ---------------- epilogue (warps 5..8 -> TMEM lane quarters 1,2,3,0)
     // Per nu tile: drain the five level accumulators of this warp's TMEM lane
     // quarter into one FP64 value per element, scaled, in the shared-memory
     // copy of G; release TMEM (the MMA warp starts the next nu tile); then
-    // contract G with the FP64 AO values while those MMAs run.
+    // contract G with the FP64 AO values while those MMAs run.  A tile's
+    // final sums are formed while the MMAs of the next tile run.
     const int quarter = warp & 3;
     const int r = quarter * 32 + lane;        // TMEM lane / G row drained by this thread
     const int role = warp - 5;                // 0..3
@@ -519,111 +583,126 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     // point contracted by this thread: NQA = 4 -> lane (all roles share the 32
     // points, each with its own AO quantities); NQA = 1 -> the role's 32 rows
     const int pc = (NQA == 4) ? lane : etid;
-    const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pc;  // element (q, k) at aop[q*ldq + k*PTS]
-    // G = 2^(e_r + f_nu - 60) sum_L acc_L 2^(48 - 8 L); the drain below forms
-    // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^16
-    const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 44);
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const uint64_t stream = policy_evict_first();
-    for (int nt = 0; nt < nnt; ++nt) {
-      const int n0 = nt * kN;
-      double* cs = s_cscale[nt & 1];
-      if (etid < kN) {
-        const int nc = n0 + etid;
-        const int nu = nc < kt ? am[nc] : -1;
-        cs[etid] = nu >= 0 ? ldexp(1.0, args.fexp[nu]) : 0.0;
+    int gnt = 0;        // nu-tile counter across tiles
+    bool stop = false;  // uniform across the four epilogue warps
+    for (int i = 0; !stop; ++i) {
+      // one reader for the four warps keeps their decisions uniform
+      if (etid == 0) {
+        s_epi_tile = read_tile(i);
+        mbar_arrive(&tile_empty_bar[i & 1]);
       }
-      // (A) column scales written; every role has finished reading sG
       asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      // uniform stop decision: the flag slot read here was written before (B)
-      // of the previous nu tile
-      if (nt > 0 && s_epi_abort[(nt - 1) & 1]) break;
-      const long long te = clock64();
-      if (!mbar_wait(&tfull_bar, nt & 1)) s_abort = 1;
-      const long long td = clock64();
-      tr0 += td - te;
-      tc_fence_after();
+      const int t = s_epi_tile;
+      if (t < 0) break;
+      const int kt = tb.kt[t];
+      const int nnt = (kt + kN - 1) / kN;
+      const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+      const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pc;  // element (q, k) at aop[q*ldq + k*PTS]
+      // G = 2^(e_r + f_nu - 60) sum_L acc_L 2^(48 - 8 L); the drain below forms
+      // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^16
+      const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 44);
+      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int nt = 0; nt < nnt; ++nt, ++gnt) {
+        const int n0 = nt * kN;
+        double* cs = s_cscale[gnt & 1];
+        if (etid < kN) {
+          const int nc = n0 + etid;
+          const int nu = nc < kt ? am[nc] : -1;
+          cs[etid] = nu >= 0 ? ldexp(1.0, args.fexp[nu]) : 0.0;
+        }
+        // (A) column scales written; every role has finished reading sG
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        // uniform stop decision: the flag slot read here was written before (B)
+        // of the previous nu tile
+        if (gnt > 0 && s_epi_abort[(gnt - 1) & 1]) { stop = true; break; }
+        const long long te = clock64();
+        if (!mbar_wait(&tfull_bar, gnt & 1)) s_abort = 1;
+        const long long td = clock64();
+        tr0 += td - te;
+        tc_fence_after();
 #pragma unroll 1
-      for (int c = 0; c < kN / 16; ++c) {
-        int32_t v[kLevels][16];
+        for (int c = 0; c < kN / 16; ++c) {
+          int32_t v[kLevels][16];
 #pragma unroll
-        for (int L = 0; L < kLevels; ++L)
-          tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + L * kN + c * 16, v[L]);
-        tmem_ld_wait();
+          for (int L = 0; L < kLevels; ++L)
+            tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + L * kN + c * 16, v[L]);
+          tmem_ld_wait();
 #pragma unroll
-        for (int L = 0; L < kLevels; ++L) after_wait16(v[L]);
+          for (int L = 0; L < kLevels; ++L) after_wait16(v[L]);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          // sum_L acc_L 2^(48 - 8 L), smallest terms first
-          double g = i32_times_pow2<0>(v[4][j]);
-          g += i32_times_pow2<8>(v[3][j]);
-          g += i32_times_pow2<16>(v[2][j]);
-          g += i32_times_pow2<24>(v[1][j]);
-          g += i32_times_pow2<32>(v[0][j]);
-          sG[(c * 16 + j) * kRows + r] = g * rowscale * cs[c * 16 + j];
+          for (int j = 0; j < 16; ++j) {
+            // sum_L acc_L 2^(48 - 8 L), smallest terms first
+            double g = i32_times_pow2<0>(v[4][j]);
+            g += i32_times_pow2<8>(v[3][j]);
+            g += i32_times_pow2<16>(v[2][j]);
+            g += i32_times_pow2<24>(v[1][j]);
+            g += i32_times_pow2<32>(v[0][j]);
+            sG[(c * 16 + j) * kRows + r] = g * rowscale * cs[c * 16 + j];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty_bar);
+        const long long tc0 = clock64();
+        tr1 += tc0 - td;
+        if (etid == 0) s_epi_abort[gnt & 1] = s_abort;
+        // (B) G of this nu tile complete in shared memory
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        const double* ao_nt = aop + (int64_t)n0 * PTS;
+        if (NQA == 4) {
+          switch (role) {
+            case 0: contract_role<0>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            case 1: contract_role<1>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            case 2: contract_role<2>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            default: contract_role<3>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+          }
+        } else {
+          // rows are points: sums over the nq_ao (1 or 4) quantities of this point
+#pragma unroll 4
+          for (int c = 0; c < kN; ++c) {
+            const double g = sG[c * kRows + etid];
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq)
+              if (qq < nq_ao) acc[qq] = fma(g, ldg_f64_stream(ao_nt + qq * ldq + c * PTS, stream), acc[qq]);
+          }
+        }
+        if (args.trace) {
+          // results of the contraction are complete when they are used
+          double chk = acc[0] + acc[1] + acc[2] + acc[3] + acc[4];
+          asm volatile("" : "+d"(chk));
+          tr2 += clock64() - tc0;
         }
       }
-      tc_fence_before();
-      mbar_arrive(&tempty_bar);
-      const long long tc0 = clock64();
-      tr1 += tc0 - td;
-      if (etid == 0) s_epi_abort[nt & 1] = s_abort;
-      // (B) G of this nu tile complete in shared memory
+      // (C) gather the per-point sums and finalise
       asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      const double* ao_nt = aop + (int64_t)n0 * PTS;
+      const bool aborted = stop || s_abort != 0;
       if (NQA == 4) {
         switch (role) {
-          case 0: contract_role<0>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-          case 1: contract_role<1>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-          case 2: contract_role<2>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-          default: contract_role<3>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+          case 0: store_role<0>(s_sums, lane, acc); break;
+          case 1: store_role<1>(s_sums, lane, acc); break;
+          case 2: store_role<2>(s_sums, lane, acc); break;
+          default: store_role<3>(s_sums, lane, acc); break;
         }
-      } else {
-        // rows are points: sums over the nq_ao (1 or 4) quantities of this point
-#pragma unroll 4
-        for (int c = 0; c < kN; ++c) {
-          const double g = sG[c * kRows + etid];
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq)
-            if (qq < nq_ao) acc[qq] = fma(g, ldg_f64_stream(ao_nt + qq * ldq + c * PTS, stream), acc[qq]);
+        asm volatile("bar.sync 1, 128;\n" ::: "memory");
+        if (role == 0 && !aborted) {
+          const int64_t oidx = tb.out[(int64_t)t * tb.TP + lane];
+          if (oidx >= 0) finalize_point_tc(s_sums[lane], 4, nq_ao, args.out, oidx, args.prm);
         }
-      }
-      if (args.trace) {
-        // results of the contraction are complete when they are used
-        double chk = acc[0] + acc[1] + acc[2] + acc[3] + acc[4];
-        asm volatile("" : "+d"(chk));
-        tr2 += clock64() - tc0;
+      } else if (!aborted) {
+        const int64_t oidx = tb.out[(int64_t)t * tb.TP + etid];
+        double s16[16];
+        for (int q = 0; q < 16; ++q) s16[q] = q < 4 ? acc[q] : 0.0;
+        if (oidx >= 0) finalize_point_tc(s16, 1, nq_ao, args.out, oidx, args.prm);
       }
     }
     if (args.trace && etid == 0) {
-      args.trace[(int64_t)t * 8 + 5] = tr0;
-      args.trace[(int64_t)t * 8 + 6] = tr1;
-      args.trace[(int64_t)t * 8 + 7] = tr2;
-    }
-    // (C) gather the per-point sums and finalise
-    asm volatile("bar.sync 1, 128;\n" ::: "memory");
-    const bool aborted = s_abort != 0;
-    if (NQA == 4) {
-      switch (role) {
-        case 0: store_role<0>(s_sums, lane, acc); break;
-        case 1: store_role<1>(s_sums, lane, acc); break;
-        case 2: store_role<2>(s_sums, lane, acc); break;
-        default: store_role<3>(s_sums, lane, acc); break;
-      }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      if (role == 0 && !aborted) {
-        const int64_t oidx = tb.out[(int64_t)t * tb.TP + lane];
-        if (oidx >= 0) finalize_point_tc(s_sums[lane], 4, nq_ao, args.out, oidx, args.prm);
-      }
-    } else if (!aborted) {
-      const int64_t oidx = tb.out[(int64_t)t * tb.TP + etid];
-      double s16[16];
-      for (int i = 0; i < 16; ++i) s16[i] = i < 4 ? acc[i] : 0.0;
-      if (oidx >= 0) finalize_point_tc(s16, 1, nq_ao, args.out, oidx, args.prm);
+      args.trace[(int64_t)blockIdx.x * 8 + 5] = tr0;
+      args.trace[(int64_t)blockIdx.x * 8 + 6] = tr1;
+      args.trace[(int64_t)blockIdx.x * 8 + 7] = tr2;
     }
   }
   __syncthreads();
-  if (args.trace && threadIdx.x == 0) args.trace[(int64_t)t * 8] = clock64() - t_start;
+  if (args.trace && threadIdx.x == 0) args.trace[(int64_t)blockIdx.x * 8] = clock64() - t_start;
   if (s_abort && threadIdx.x == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
   if (warp == 4) {
     // every MMA this thread issued has completed before TMEM is released
@@ -710,16 +789,78 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
   return CTC_OK;
 }
 
-int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
-                       int32_t** eexp) {
-  const size_t plane_bytes = (size_t)tb.C * kPlanes * kRows * tb.Kcap;
-  const size_t need = plane_bytes + 256 + sizeof(int32_t) * (size_t)tb.C * kRows;
-  int rc = mol->ws_sl.ensure(need, st);
+// Chunk workspace of the tensor-core path, one layout for both users (the AO
+// kernel that writes the digit planes and the contraction):
+//   planes [C][4][128][Kcap] int8 | eexp [C][128] | tile order: keys in/out,
+//   ids in, order [C] | tile counter | radix-sort temporary storage
+struct TcWorkspace {
+  int8_t* planes;
+  int32_t* eexp;
+  uint32_t* keys_in;
+  uint32_t* keys_out;
+  int32_t* ids;
+  int32_t* order;
+  int32_t* counter;
+  void* sort_tmp;
+  size_t sort_bytes;
+};
+
+int tc_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, TcWorkspace* w) {
+  size_t sort_bytes = 0;
+  CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t*)nullptr,
+                                               (uint32_t*)nullptr, (int32_t*)nullptr,
+                                               (int32_t*)nullptr, tb.C, 0, 15, st));
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_planes = take((size_t)tb.C * kPlanes * kRows * tb.Kcap);
+  const size_t o_eexp = take(sizeof(int32_t) * (size_t)tb.C * kRows);
+  const size_t o_kin = take(sizeof(uint32_t) * tb.C);
+  const size_t o_kout = take(sizeof(uint32_t) * tb.C);
+  const size_t o_ids = take(sizeof(int32_t) * tb.C);
+  const size_t o_order = take(sizeof(int32_t) * tb.C);
+  const size_t o_counter = take(sizeof(int32_t));
+  const size_t o_tmp = take(sort_bytes);
+  int rc = mol->ws_sl.ensure(off, st);
   if (rc != CTC_OK) return rc;
-  *planes = (int8_t*)mol->ws_sl.p;
-  *eexp = (int32_t*)((char*)mol->ws_sl.p + (plane_bytes + 255) / 256 * 256);
+  char* base = (char*)mol->ws_sl.p;
+  w->planes = (int8_t*)(base + o_planes);
+  w->eexp = (int32_t*)(base + o_eexp);
+  w->keys_in = (uint32_t*)(base + o_kin);
+  w->keys_out = (uint32_t*)(base + o_kout);
+  w->ids = (int32_t*)(base + o_ids);
+  w->order = (int32_t*)(base + o_order);
+  w->counter = (int32_t*)(base + o_counter);
+  w->sort_tmp = base + o_tmp;
+  w->sort_bytes = sort_bytes;
   return CTC_OK;
 }
+
+int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
+                       int32_t** eexp) {
+  TcWorkspace w;
+  const int rc = tc_workspace(mol, tb, st, &w);
+  if (rc != CTC_OK) return rc;
+  *planes = w.planes;
+  *eexp = w.eexp;
+  return CTC_OK;
+}
+
+namespace {
+// sort keys: largest compact K first (ascending kMaxKt - kt), ids = tile index
+__global__ void tile_order_keys_kernel(const int32_t* __restrict__ kt, int C, uint32_t* keys,
+                                       int32_t* ids, int32_t* counter) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *counter = 0;
+  if (i < C) {
+    keys[i] = (uint32_t)(kMaxKt - min(kt[i], kMaxKt));
+    ids[i] = i;
+  }
+}
+}  // namespace
 
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
@@ -730,9 +871,14 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   if (rc != CTC_OK) return rc;
   // int8 planes of the tile rows + row exponents, written by this chunk's AO
   // kernel (launch_ao_tiles_sliced)
-  int8_t* planes = nullptr;
-  int32_t* eexp = nullptr;
-  if ((rc = tc_slice_workspace(mol, tb, st, &planes, &eexp)) != CTC_OK) return rc;
+  TcWorkspace w;
+  if ((rc = tc_workspace(mol, tb, st, &w)) != CTC_OK) return rc;
+  // persistent CTAs take the chunk's tiles largest first, so the last tiles
+  // handed out are the cheapest ones
+  tile_order_keys_kernel<<<(tb.C + 255) / 256, 256, 0, st>>>(tb.kt, tb.C, w.keys_in, w.ids, w.counter);
+  CTC_CUDA_TRY(cudaGetLastError());
+  CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.keys_in, w.keys_out, w.ids,
+                                               w.order, tb.C, 0, 15, st));
   // tensor map over the planes: 2-D, rows = C*4*128, inner = Kcap bytes
   PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode();
   if (!enc) return fail(CTC_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
@@ -741,25 +887,34 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   cuuint64_t gstride[1] = {(cuuint64_t)tb.Kcap};
   cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kRows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult cr = enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, planes, gdim, gstride, box, estr,
+  CUresult cr = enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, w.planes, gdim, gstride, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return fail(CTC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)cr));
+  static int num_sms = 0;
+  if (num_sms == 0) {
+    int dev = 0;
+    CTC_CUDA_TRY(cudaGetDevice(&dev));
+    CTC_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  const int grid = std::min(tb.C, num_sms);
   TcArgs a;
   a.tb = tb;
   a.nqa = plan.nqa;
   a.Dp = (const uint32_t*)mol->d_Dsl;
   a.fexp = (const int32_t*)mol->d_Dscale;
-  a.eexp = eexp;
+  a.eexp = w.eexp;
   a.Mpad = mol->Mpad;
   a.out = *out;
   a.prm = *prm;
   a.status = mol->d_status;
+  a.order = w.order;
+  a.tile_counter = w.counter;
   a.trace = nullptr;
-  // CTC_TC_TRACE=1: per-tile cycle counters of the kernel's roles, summarised
+  // CTC_TC_TRACE=1: per-CTA cycle counters of the kernel's roles, summarised
   // on stderr after each launch (synchronises the stream; diagnostics only)
   static const bool trace_on = std::getenv("CTC_TC_TRACE") != nullptr;
-  if (trace_on) CTC_CUDA_TRY(cudaMallocAsync((void**)&a.trace, sizeof(long long) * 8 * tb.C, st));
+  if (trace_on) CTC_CUDA_TRY(cudaMallocAsync((void**)&a.trace, sizeof(long long) * 8 * grid, st));
   static bool attr[2] = {false, false};
   ProfScope ps(mol, 0, st);
   if (plan.nqa == 4) {
@@ -767,36 +922,40 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
       CTC_CUDA_TRY(cudaFuncSetAttribute(tc_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc));
       attr[1] = true;
     }
-    tc_tile_kernel<4><<<tb.C, kThreadsTc, kSmemTc, st>>>(amap, a);
+    tc_tile_kernel<4><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
   } else {
     if (!attr[0]) {
       CTC_CUDA_TRY(cudaFuncSetAttribute(tc_tile_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc));
       attr[0] = true;
     }
-    tc_tile_kernel<1><<<tb.C, kThreadsTc, kSmemTc, st>>>(amap, a);
+    tc_tile_kernel<1><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
   }
   CTC_CUDA_TRY(cudaGetLastError());
   if (trace_on) {
-    std::vector<long long> tr((size_t)8 * tb.C);
+    std::vector<long long> tr((size_t)8 * grid);
     std::vector<int32_t> kt(tb.C);
     CTC_CUDA_TRY(cudaMemcpyAsync(tr.data(), a.trace, sizeof(long long) * tr.size(), cudaMemcpyDeviceToHost, st));
     CTC_CUDA_TRY(cudaMemcpyAsync(kt.data(), tb.kt, sizeof(int32_t) * tb.C, cudaMemcpyDeviceToHost, st));
     CTC_CUDA_TRY(cudaStreamSynchronize(st));
     CTC_CUDA_TRY(cudaFreeAsync(a.trace, st));
-    double sum[8] = {0}, stages = 0, ktmax = 0, ktsum = 0;
-    for (int i = 0; i < tb.C; ++i) {
+    double sum[8] = {0}, stages = 0, ktmax = 0, ktsum = 0, totmax = 0;
+    for (int i = 0; i < grid; ++i) {
       for (int k = 0; k < 8; ++k) sum[k] += (double)tr[(size_t)8 * i + k];
+      totmax = std::max(totmax, (double)tr[(size_t)8 * i]);
+    }
+    for (int i = 0; i < tb.C; ++i) {
       const double nk = kt[i] / (double)kBK;
       stages += nk * nk;
       ktsum += kt[i];
       ktmax = std::max(ktmax, (double)kt[i]);
     }
     std::fprintf(stderr,
-                 "[ctc tc trace] tiles %d mean kt %.0f max kt %.0f | cycles per stage: total %.0f "
-                 "prod_wait_empty %.0f prod_work %.0f mma_wait_full %.0f mma_wait_tempty %.0f "
-                 "epi_wait_tfull %.0f epi_drain %.0f epi_contract %.0f\n",
-                 tb.C, ktsum / tb.C, ktmax, sum[0] / stages, sum[1] / stages, sum[2] / stages,
-                 sum[3] / stages, sum[4] / stages, sum[5] / stages, sum[6] / stages, sum[7] / stages);
+                 "[ctc tc trace] tiles %d CTAs %d mean kt %.0f max kt %.0f | CTA cycles mean %.0f max %.0f | "
+                 "per stage: total %.0f prod_wait_empty %.0f prod_work %.0f mma_wait_full %.0f "
+                 "mma_wait_tempty %.0f epi_wait_tfull %.0f epi_drain %.0f epi_contract %.0f\n",
+                 tb.C, grid, ktsum / tb.C, ktmax, sum[0] / grid, totmax, sum[0] / stages,
+                 sum[1] / stages, sum[2] / stages, sum[3] / stages, sum[4] / stages, sum[5] / stages,
+                 sum[6] / stages, sum[7] / stages);
   }
   return CTC_OK;
 }
