@@ -161,6 +161,8 @@ def load_lib():
     lib.ctc_molecule_get_stats.argtypes = [vp, vp]
     lib.ctc_molecule_reset_stats.argtypes = [vp]
     lib.ctc_molecule_set_profiling.argtypes = [vp, i32]
+    lib.ctc_eval_local.argtypes = [vp, vp, i64, i32, vp, vp, vp]
+    lib.ctc_adjoint.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp]
     return lib
 
 
@@ -472,6 +474,218 @@ def run_reference(args, ws, rank):
 
 
 # --------------------------------------------------------------------------- main
+# --------------------------------------------------------------------------- other configurations
+PARITY_ATOL = 1e-14
+
+
+def _sample_errors(got, ref, scale, keys, atol=PARITY_ATOL):
+    """Largest (|got - ref| - atol) / scale per key over a point sample (scale: sum of
+    |terms|); the absolute floor atol covers points where every AO is screened out
+    and the result is exactly 0 (the test suite's criterion |got - ref| <= tol scale + atol)."""
+    out = {}
+    for k in keys:
+        g, r, sc = np.asarray(got[k]), np.asarray(ref[k]), np.asarray(scale[k])
+        out[k] = float((np.maximum(np.abs(g - r) - atol, 0.0) / np.maximum(sc, 1e-300)).max())
+    return out
+
+
+def _timed(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _local_outputs(n, keys):
+    import torch
+    outs = {k: torch.empty(n * WIDTH[k], dtype=torch.float64, device="cuda") for k in keys}
+    return outs, Outputs(**{k: outs[k].data_ptr() for k in keys})
+
+
+def _to_host(outs, n):
+    res = {}
+    for k, t in outs.items():
+        a = t.cpu().numpy()
+        res[k] = a.reshape(n, 3) if k == "grad" else (a.reshape(n, 3, 3) if k == "hess" else a)
+    return res
+
+
+def run_workload(args):
+    """One JSON line for a configuration other than the headline one.
+
+    c1: 12-atom molecule (Cartesian up to d), 1e5 points uniform in the box + 4 bohr, rho only,
+        FP64 form and tensor-core form.
+    c3: 60-atom molecule (up to d), atom-centred grid of 75 radial x 308 angular points per atom
+        with Becke weights (~1.4e6 points); one step = forward (rho, grad rho), the GGA functional
+        L = sum w (c1 rho^4/3 + c2 |grad rho|^2 / rho^4/3) and its adjoint (dL/dD, dL/dR);
+        checked against central differences (h = 1e-5) on 20 symmetric D pairs and 4 atoms.
+    c4: 1000-atom molecule (Cartesian up to g, D zeroed beyond 12 bohr), 368^3 cube at 0.25 bohr
+        (4.98e7 points), rho + grad rho + lap rho on the tensor-core path.
+    c5: 100-atom molecule (up to d), electrostatic potential on its four nested surfaces.
+    Parity fields: largest error over a point sample relative to the sum of absolute terms
+    (the measure of tests/helpers.py), against the FP64 oracle.
+    """
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import term_scales
+    from oracle import oracle as O
+    lib = load_lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    prm = Params(ALPHA, 1 / 9, 1 / 6, 1.0)
+    w = args.workload
+    line = {"impl": "ours", "workload_id": w, "n_gpus": 1, "data": "synthetic"}
+    if w == "c1":
+        mol = S.make_molecule("c1", seed=0)
+        pts = S.random_points(np.random.default_rng(1), mol, 100000, pad=4.0)
+        n = len(pts)
+        h = create(lib, mol)
+        dp = torch.as_tensor(pts, device="cuda")
+        outs, o = _local_outputs(n, ("rho",))
+        vals = {}
+        for name, prec in (("fp64", 0), ("tc", 1)):
+            def fn(p=prec):
+                check(lib, lib.ctc_eval_local(h, dp.data_ptr(), n, p, C.byref(prm), C.byref(o), stream), "c1")
+            ms = _timed(fn, args.steps, args.warmup)
+            fn()
+            torch.cuda.synchronize()
+            got = _to_host(outs, n)
+            idx = np.random.default_rng(2).choice(n, 512, replace=False)
+            ref = O.eval_local(mol.flat(), mol.D, pts[idx], keys=("rho",))
+            sc = term_scales(mol.flat(), mol.D, pts[idx])
+            vals[name] = {"value": n / (ms * 1e-3), "ms_per_step": ms,
+                          "max_err_rel_sum_abs": _sample_errors({"rho": got["rho"][idx]}, ref, sc, ("rho",))}
+        line.update({"metric": "grid pts/s for rho (12-atom molecule, 1e5 points)", "value": vals["fp64"]["value"],
+                     "unit": "grid points/s", "higher_is_better": True, "dtype": "f64",
+                     "config": {"workload": "c1: 12 atoms, Cartesian up to d, 1e5 uniform points, rho only",
+                                "nbasis": mol.nbasis, "points": n},
+                     "fp64_form": vals["fp64"], "tc_form": vals["tc"]})
+        lib.ctc_molecule_destroy(h)
+    elif w == "c3":
+        from chemtoolscuda_b200 import molecule_from_synthetic
+        from chemtoolscuda_b200.autograd import density_and_gradient, gga_functional
+        mol = S.make_molecule("c3", seed=0)
+        grid, wts = S.atom_grid(mol, nrad=75, ntheta=14, nphi=22)
+        n = len(grid)
+        pm = molecule_from_synthetic(mol)
+        pts = torch.as_tensor(grid, device="cuda")
+        wt = torch.as_tensor(wts, device="cuda")
+        D = torch.as_tensor(mol.D, device="cuda").requires_grad_(True)
+        R = torch.as_tensor(mol.coords).clone().requires_grad_(True)
+
+        def L(Dm, Rm):
+            rho, grad = density_and_gradient(pm, pts, Dm, Rm)
+            return gga_functional(rho, grad, wt)
+
+        def step():
+            D.grad = None
+            R.grad = None
+            L(D, R).backward()
+        ms = _timed(step, args.steps, args.warmup)
+        step()
+        gD = D.grad.cpu().numpy()
+        gR = R.grad.numpy()
+        hfd = 1e-5
+        rng = np.random.default_rng(1)
+        M = mol.nbasis
+        pairs = [(int(a), int(b)) for a, b in rng.integers(0, M, size=(20, 2))]
+        errD = 0.0
+        with torch.no_grad():
+            for a, b in pairs:
+                Dp, Dn = D.detach().clone(), D.detach().clone()
+                Dp[a, b] += hfd
+                Dn[a, b] -= hfd
+                if a != b:
+                    Dp[b, a] += hfd
+                    Dn[b, a] -= hfd
+                fd = (L(Dp, R.detach()).item() - L(Dn, R.detach()).item()) / (2 * hfd)
+                an = gD[a, b] + (gD[b, a] if a != b else 0.0)
+                errD = max(errD, abs(an - fd))
+            errR = 0.0
+            for A in range(4):
+                for j in range(3):
+                    Rp, Rn = R.detach().clone(), R.detach().clone()
+                    Rp[A, j] += hfd
+                    Rn[A, j] -= hfd
+                    fd = (L(D.detach(), Rp).item() - L(D.detach(), Rn).item()) / (2 * hfd)
+                    errR = max(errR, abs(gR[A, j] - fd))
+        line.update({"metric": "grid pts/s for forward (rho, grad rho) + adjoint (dL/dD, dL/dR) of a GGA functional",
+                     "value": n / (ms * 1e-3), "unit": "grid points/s", "ms_per_step": ms,
+                     "higher_is_better": True, "dtype": "f64",
+                     "config": {"workload": "c3: 60 atoms (up to d), 75 x 308 points per atom, Becke weights",
+                                "nbasis": M, "points": n},
+                     "finite_differences": {"h": hfd, "D_pairs": 20, "atoms": 4,
+                                            "max_err_dLdD_rel_max": errD / max(np.abs(gD).max(), 1e-300),
+                                            "max_err_dLdR_rel_max": errR / max(np.abs(gR).max(), 1e-300)}})
+    elif w == "c4":
+        mol = S.make_molecule("c4", seed=0, device="cuda")
+        shape = (368, 368, 368)
+        origin, axes = S.cube_grid(mol, 0.25, shape)
+        n = int(np.prod(shape))
+        h = create(lib, mol)
+        check(lib, lib.ctc_molecule_prepare(h, 1), "prepare")
+        keys = ("rho", "grad", "lap")
+        outs, o = _local_outputs(n, keys)
+        org = np.ascontiguousarray(origin)
+        ax = np.ascontiguousarray(axes)
+        sh = np.ascontiguousarray(np.array(shape, dtype=np.int32))
+
+        def fn():
+            check(lib, lib.ctc_eval_cubic(h, org.ctypes.data, ax.ctypes.data, sh.ctypes.data, 1,
+                                          C.byref(prm), C.byref(o), stream), "c4")
+        ms = _timed(fn, max(1, min(args.steps, 2)), 1)
+        st = stats(lib, h)
+        got = _to_host(outs, n)
+        rng = np.random.default_rng(3)
+        allp = S.cube_points(origin, axes, shape)
+        # sample points where the density is not negligible, plus a few anywhere
+        dense = np.nonzero(got["rho"] > 1e-6)[0]
+        idx = np.concatenate([rng.choice(dense, 40, replace=False), rng.choice(n, 8, replace=False)])
+        ref = O.eval_local(mol.flat(), mol.D, allp[idx], keys=keys)
+        sc = term_scales(mol.flat(), mol.D, allp[idx])
+        err = _sample_errors({k: got[k][idx] for k in keys}, ref, sc, keys)
+        line.update({"metric": "grid pts/s for rho, grad rho, lap rho (1000-atom molecule, tensor-core path)",
+                     "value": n / (ms * 1e-3), "unit": "grid points/s", "ms_per_step": ms,
+                     "higher_is_better": True, "dtype": "int8x4 split operands, exact int32 accumulation, fp64 AO/epilogue",
+                     "config": {"workload": "c4: 1000 atoms, Cartesian up to g, D zeroed beyond 12 bohr, 368^3 cube at 0.25 bohr",
+                                "nbasis": mol.nbasis, "points": n,
+                                "mean_compact_aos_per_tile": st[2] / max(st[0], 1)},
+                     "parity": {"sample_points": int(len(idx)), "max_err_rel_sum_abs": err, "tolerance": 1e-8,
+                                "atol": PARITY_ATOL}})
+        lib.ctc_molecule_destroy(h)
+    elif w == "c5":
+        mol = S.make_molecule("c5", seed=0)
+        sp = S.surface_points(mol, seed=0)
+        n = len(sp)
+        h = create(lib, mol)
+        dp = torch.as_tensor(np.ascontiguousarray(sp), device="cuda")
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+
+        def fn():
+            check(lib, lib.ctc_eval_esp(h, dp.data_ptr(), n, out.data_ptr(), stream), "esp")
+        ms = _timed(fn, max(1, min(args.steps, 2)), 1)
+        got = out.cpu().numpy()
+        idx = np.random.default_rng(4).choice(n, 64, replace=False)
+        ref = O.eval_esp(mol.flat(), mol.D, mol.coords, mol.charges, sp[idx])
+        rel = float((np.abs(got[idx] - ref) / np.maximum(np.abs(ref), 1e-300)).max())
+        line.update({"metric": "ESP points/s (100-atom molecule, four nested surfaces)",
+                     "value": n / (ms * 1e-3), "unit": "ESP points/s", "ms_per_step": ms,
+                     "higher_is_better": True, "dtype": "f64",
+                     "config": {"workload": "c5: 100 atoms (up to d), surfaces at 1.4/1.6/1.8/2.0 x radius, 20 points/bohr^2",
+                                "nbasis": mol.nbasis, "points": n},
+                     "parity": {"sample_points": 64, "max_rel_err": rel, "tolerance": 1e-8}})
+        lib.ctc_molecule_destroy(h)
+    else:
+        raise SystemExit(f"unknown workload {w}")
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,8 +701,17 @@ def main():
     ap.add_argument("--cpu-points", type=int, default=1500)
     ap.add_argument("--esp-points", type=int, default=20000)
     ap.add_argument("--ref-points", type=int, default=16384)
+    ap.add_argument("--workload", default=None, choices=["c1", "c3", "c4", "c5"],
+                    help="measure another configuration instead of the headline one (one GPU)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
+    if args.workload is not None:
+        if rank == 0:
+            print(json.dumps(run_workload(args)), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
     if args.impl == "reference":
         line = run_reference(args, ws, rank)
         if rank == 0:

@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kSliceThreads)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t ld_q = (int64_t)TP * tb.Kcap;
   const double* A = tb.ao + (int64_t)t * tb.nq * ld_q;
-  int8_t* P = planes + (int64_t)t * kSplitPlanes * kSplitRows * tb.Kcap;
+  int8_t* P = planes + (int64_t)t * kSplitPlanesA * kSplitRows * tb.Kcap;
   const int nchunk = min(kt - kbeg, kSliceCols) / 32;
   const int nitem = (kSplitRows / 32) * nchunk;  // warp-sized items
   for (int it = warp; it < nitem; it += kSliceThreads / 32) {
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kSliceThreads)
     const int r = rg * 32 + lane;
     const int q = nqa == 4 ? rg : 0;
     const int p = nqa == 4 ? lane : r;
-    const double f = split_row_factor(eexp[(int64_t)t * kSplitRows + r]);
+    const double f = split_row_factor(eexp[(int64_t)t * kSplitRows + r], kFixedBitsA);
     const double* col = A + q * ld_q + p + (int64_t)(c * 32) * TP;
     write_row_digits32([&](int i) { return __ldg(col + (int64_t)i * TP); }, f, P, r, tb.Kcap, c * 32);
   }

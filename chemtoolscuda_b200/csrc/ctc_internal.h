@@ -154,7 +154,7 @@ namespace ctc {
 int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cudaStream_t st);
 // Same, and in the same kernel the int8 digit planes of the tile rows
 // (nqa = 4: 32 points x {phi, d phi}; nqa = 1: 128 points x phi) with one
-// exponent per row, for the tensor-core split path: planes [C][4][128][Kcap],
+// exponent per row, for the tensor-core split path: planes [C][5][128][Kcap],
 // eexp [C][128].
 int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
                            int8_t* planes, int32_t* eexp, cudaStream_t st);

@@ -1,25 +1,34 @@
 // ctc_split.cuh -- the INT8 digit split shared by the operand producers
 // (D in ctc_tc.cu, the tile rows in the AO kernel of ctc_ao.cu).
 //
-// A row of values x_k (a tile row of phi or d_k phi over the tile's compact
-// AOs, or a row of D) is scaled by 2^-e, e the exponent of its largest |x|
-// (|x| < 2^e), and rounded to the 31-bit fixed-point integer
-// I = rint(x 2^(30-e)), |I| <= 2^30.  I is written as four balanced base-256
-// digits d_0..d_3, |d_i| <= 128, I = sum_i d_i 256^(3-i): one int8 plane per
-// digit, most significant first.
+// A row of values x_k is scaled by 2^-e, e the exponent of its largest |x|
+// (|x| < 2^e), and rounded to a fixed-point integer written in balanced
+// base-256 digits (|d| <= 128), one int8 plane per digit, most significant
+// first:
+//   * D rows (B operand): I = rint(x 2^(30-e)), |I| <= 2^30, four digits;
+//   * tile rows of phi and grad phi (A operand): I = rint(x 2^(38-e)),
+//     |I| <= 2^38, five digits.
+// The A rows get the extra digit because a row's error is set by its largest
+// entry: an AO row with one steep function (a tight g shell near its centre)
+// and many small ones loses relative precision on the small ones, which
+// showed as errors of 2e-8 of the sum of absolute terms with 31 bits; D rows
+// do not have this spread.
 #pragma once
 
 #include <cstdint>
 
 namespace ctc {
 
-constexpr int kSplitPlanes = 4;   // digit planes per operand
+constexpr int kSplitPlanesD = 4;  // digit planes of D (B operand)
+constexpr int kSplitPlanesA = 5;  // digit planes of the tile rows (A operand)
 constexpr int kSplitRows = 128;   // rows of a tile operand (MMA M)
+constexpr int kFixedBitsD = 30;   // |I| <= 2^30
+constexpr int kFixedBitsA = 38;   // |I| <= 2^38
 
-// Lowest row exponent used: rows whose largest |x| is below 2^-990 are
-// scaled as if it were 2^-990 (their digits are then zero), so that the row
-// factor 2^(30 - e) stays a normal double.
-constexpr int kMinScaleExponent = -990;
+// Lowest row exponent used: rows whose largest |x| is below 2^-980 are
+// scaled as if it were 2^-980 (their digits are then zero), so that the row
+// factors 2^(bits - e) stay normal doubles.
+constexpr int kMinScaleExponent = -980;
 
 // balanced base-256 digits of |I| <= 2^30, packed in a word: byte p holds the
 // digit of weight 256^(3-p) (byte 0 = the most significant digit).  Adding
@@ -38,9 +47,15 @@ __device__ __forceinline__ int32_t rint_i32(double y) {
   return __double2loint(y + 6755399441055744.0);
 }
 
-// 2^(30 - e): the factor that maps a row with |x| < 2^e onto |I| <= 2^30
-__device__ __forceinline__ double split_row_factor(int e) {
-  return __longlong_as_double((long long)(30 - e + 1023) << 52);
+// rint(y) for |y| < 2^51 as int64 (round half to even): the low 52 bits of
+// y + 1.5 * 2^52 hold 2^51 + rint(y).
+__device__ __forceinline__ long long rint_i64(double y) {
+  return __double_as_longlong(y + 6755399441055744.0) - 0x4338000000000000LL;
+}
+
+// 2^(bits - e): the factor that maps a row with |x| < 2^e onto |I| <= 2^bits
+__device__ __forceinline__ double split_row_factor(int e, int bits) {
+  return __longlong_as_double((long long)(bits - e + 1023) << 52);
 }
 
 __device__ __forceinline__ int scale_exponent(double amax) {
@@ -63,25 +78,33 @@ __device__ __forceinline__ void transpose_bytes4x4(uint32_t a, uint32_t b, uint3
   out[3] = __byte_perm(t2, t3, 0x7632);           // a3 b3 c3 d3
 }
 
-// Writes 32 consecutive K entries of one tile row into the four planes
+// Writes 32 consecutive K entries of one tile row into the five A planes
 // [plane][row][Kcap] (32 bytes per plane): x(i) returns the row's value at
-// K index k0 + i, f = split_row_factor(e) of the row.
+// K index k0 + i, f = split_row_factor(e, kFixedBitsA) of the row.  The four
+// most significant digits go through pack_digits, the fifth is the balanced
+// low byte.
 template <class F>
 __device__ __forceinline__ void write_row_digits32(F x, double f, int8_t* __restrict__ P, int row,
                                                    int64_t Kcap, int k0) {
-  uint32_t pw[kSplitPlanes][8];
+  uint32_t pw[kSplitPlanesA][8];
 #pragma unroll
   for (int g = 0; g < 8; ++g) {
-    uint32_t w[4];
+    uint32_t w[4], lo = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) w[i] = pack_digits(rint_i32(x(4 * g + i) * f));
+    for (int i = 0; i < 4; ++i) {
+      const long long I = rint_i64(x(4 * g + i) * f);
+      const int32_t d4 = (int32_t)(((I + 128) & 255) - 128);
+      w[i] = pack_digits((int32_t)((I - d4) >> 8));
+      lo |= (uint32_t)(d4 & 255) << (8 * i);
+    }
     uint32_t pl[4];
     transpose_bytes4x4(w[0], w[1], w[2], w[3], pl);
 #pragma unroll
-    for (int p = 0; p < kSplitPlanes; ++p) pw[p][g] = pl[p];
+    for (int p = 0; p < 4; ++p) pw[p][g] = pl[p];
+    pw[4][g] = lo;
   }
 #pragma unroll
-  for (int p = 0; p < kSplitPlanes; ++p) {
+  for (int p = 0; p < kSplitPlanesA; ++p) {
     uint4* dst = reinterpret_cast<uint4*>(P + ((int64_t)p * kSplitRows + row) * Kcap + k0);
     dst[0] = make_uint4(pw[p][0], pw[p][1], pw[p][2], pw[p][3]);
     dst[1] = make_uint4(pw[p][4], pw[p][5], pw[p][6], pw[p][7]);

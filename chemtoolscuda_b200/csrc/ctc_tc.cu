@@ -2,27 +2,27 @@
 //
 // G_t = A_t D[S_t, S_t] of the screened tile pipeline (ctc_local.cu) on the
 // 5th-generation tensor cores with results equal to the FP64 contraction to
-// ~2e-9 relative (measured on the 200-atom benchmark molecule against the
-// FP64 oracle; 1e-8 is the target).
+// ~1e-9 of the sum of absolute terms (measured against the FP64 oracle;
+// 1e-8 is the target).
 //
-// Split (an Ozaki-type scheme with exact integer accumulation):
-//   * every A row r is scaled by 2^-e_r (e_r from the row's largest |value|),
-//     every D row nu by 2^-f_nu, and rounded to a 31-bit fixed-point integer
-//     I = rint(x 2^30);
-//   * I is written in balanced base-256 digits d_0..d_3 (|d_i| <= 128,
-//     I = sum_i d_i 256^(3-i)), one int8 plane per digit;
-//   * the 13 digit products with i + j <= 4 are accumulated on INT8 tensor
+// Split (an Ozaki-type scheme with exact integer accumulation, ctc_split.cuh):
+//   * every A row r is scaled by 2^-e_r (e_r from the row's largest |value|)
+//     and rounded to I_A = rint(x 2^(38 - e_r)), five balanced base-256 digits
+//     a_0..a_4 (|a_i| <= 128, I_A = sum_i a_i 256^(4-i)); every D row nu by
+//     2^-f_nu, I_D = rint(y 2^(30 - f_nu)), four digits b_0..b_3; one int8
+//     plane per digit;
+//   * the 14 digit products with i + j <= 4 are accumulated on INT8 tensor
 //     cores (tcgen05.mma kind::i8, int32 accumulators in TMEM), one TMEM
 //     accumulator per level L = i + j;  int32 accumulation is exact as long
 //     as the compact K of a tile stays below 16 384;
-//   * the epilogue forms G = 2^(e_r + f_nu - 60) sum_L acc_L 2^(48 - 8 L) in
+//   * the epilogue forms G = 2^(e_r + f_nu - 68) sum_L acc_L 2^(56 - 8 L) in
 //     FP64 and reduces it against the FP64 AO values (same epilogue sums as
 //     the FP64 path).
-// The dropped products (i + j >= 5) are below 2^-40 of the row/column scale.
+// The dropped products (i + j >= 5) are below 2^-36 of the row/column scale.
 //
 // Kernel roles (288 threads, one persistent CTA per SM taking the chunk's
 // tiles largest first from a launch-wide counter): warps 0-3 produce the
-// operands of each K block (one thread issues the TMA loads of the four A
+// operands of each K block (one thread issues the TMA loads of the five A
 // planes; all 128 threads gather the four D planes by compact index from the
 // packed copy of D and write them in the 64-byte-swizzled K-major layout),
 // warp 4 issues the MMAs from one thread and commits them to mbarriers, warps
@@ -53,13 +53,14 @@ namespace {
 
 constexpr int kN = 64;          // nu columns per TMEM accumulator
 constexpr int kBK = 64;         // K bytes per pipeline stage
-constexpr int kStages = 3;
+constexpr int kStages = 2;
 constexpr int kRows = kSplitRows;  // tile rows (MMA M)
 constexpr int kLevels = 5;
-constexpr int kPlanes = kSplitPlanes;
+constexpr int kPlanesA = kSplitPlanesA;  // A digit planes (tile rows)
+constexpr int kPlanes = kSplitPlanesD;   // D digit planes
 constexpr int kAPlaneBytes = kRows * kBK;       // 8 KB
 constexpr int kBPlaneBytes = kN * kBK;          // 4 KB
-constexpr int kAStageBytes = kPlanes * kAPlaneBytes;
+constexpr int kAStageBytes = kPlanesA * kAPlaneBytes;
 constexpr int kBStageBytes = kPlanes * kBPlaneBytes;
 constexpr int kGBytes = kN * kRows * 8;         // FP64 copy of one nu tile of G (64 KB)
 constexpr int kSmemTc = kStages * (kAStageBytes + kBStageBytes) + kGBytes + 1024;  // + alignment slack
@@ -318,7 +319,7 @@ __global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint32_t*
   __syncthreads();
   const int e = scale_exponent(red[0]);
   if (threadIdx.x == 0) fexp[row] = e;
-  const double f = split_row_factor(e);
+  const double f = split_row_factor(e, kFixedBitsD);
   for (int k = threadIdx.x; k < Mpad; k += blockDim.x)
     Dp[(int64_t)row * Mpad + k] = pack_digits(rint_i32(d[k] * f));
 }
@@ -483,9 +484,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         tr0 += clock64() - tw;
         if (tid == 0) {
           mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
-          for (int p = 0; p < kPlanes; ++p)
+          for (int p = 0; p < kPlanesA; ++p)
             tma_load_2d_hint(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0,
-                             (t * kPlanes + p) * kRows, &full_bar[s], keep);
+                             (t * kPlanesA + p) * kRows, &full_bar[s], keep);
         }
         uint8_t* b = sB + s * kBStageBytes;
 #pragma unroll
@@ -539,7 +540,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 #pragma unroll
             for (int ks = 0; ks < kBK / 32; ++ks) {
 #pragma unroll
-              for (int pa = 0; pa < kPlanes; ++pa) {
+              for (int pa = 0; pa < kPlanesA; ++pa) {
 #pragma unroll
                 for (int pb = 0; pb < kPlanes; ++pb) {
                   const int L = pa + pb;
@@ -599,8 +600,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       const int nnt = (kt + kN - 1) / kN;
       const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
       const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pc;  // element (q, k) at aop[q*ldq + k*PTS]
-      // G = 2^(e_r + f_nu - 60) sum_L acc_L 2^(48 - 8 L); the drain below forms
-      // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^16
+      // G = 2^(e_r + f_nu - 68) sum_L acc_L 2^(56 - 8 L); the drain below forms
+      // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^24
       const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 44);
       double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
       for (int nt = 0; nt < nnt; ++nt, ++gnt) {
@@ -632,7 +633,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           for (int L = 0; L < kLevels; ++L) after_wait16(v[L]);
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            // sum_L acc_L 2^(48 - 8 L), smallest terms first
+            // sum_L acc_L 2^(32 - 8 L), smallest terms first
             double g = i32_times_pow2<0>(v[4][j]);
             g += i32_times_pow2<8>(v[3][j]);
             g += i32_times_pow2<16>(v[2][j]);
@@ -791,7 +792,7 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
 
 // Chunk workspace of the tensor-core path, one layout for both users (the AO
 // kernel that writes the digit planes and the contraction):
-//   planes [C][4][128][Kcap] int8 | eexp [C][128] | tile order: keys in/out,
+//   planes [C][5][128][Kcap] int8 | eexp [C][128] | tile order: keys in/out,
 //   ids in, order [C] | tile counter | radix-sort temporary storage
 struct TcWorkspace {
   int8_t* planes;
@@ -816,7 +817,7 @@ int tc_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, TcWork
     off = (off + bytes + 255) / 256 * 256;
     return o;
   };
-  const size_t o_planes = take((size_t)tb.C * kPlanes * kRows * tb.Kcap);
+  const size_t o_planes = take((size_t)tb.C * kPlanesA * kRows * tb.Kcap);
   const size_t o_eexp = take(sizeof(int32_t) * (size_t)tb.C * kRows);
   const size_t o_kin = take(sizeof(uint32_t) * tb.C);
   const size_t o_kout = take(sizeof(uint32_t) * tb.C);
@@ -883,7 +884,7 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode();
   if (!enc) return fail(CTC_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   CUtensorMap amap;
-  cuuint64_t gdim[2] = {(cuuint64_t)tb.Kcap, (cuuint64_t)tb.C * kPlanes * kRows};
+  cuuint64_t gdim[2] = {(cuuint64_t)tb.Kcap, (cuuint64_t)tb.C * kPlanesA * kRows};
   cuuint64_t gstride[1] = {(cuuint64_t)tb.Kcap};
   cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kRows};
   cuuint32_t estr[2] = {1, 1};

@@ -153,10 +153,21 @@ def make_basis(rng, coords, numbers, recipe, kmin=3, kmax=6, emin=0.08, emax=5e3
     return shells
 
 
-def make_density_matrix(rng, M: int, nocc: int) -> np.ndarray:
-    """D = 2 C C^T with C an M x nocc block with orthonormal columns."""
+def make_density_matrix(rng, M: int, nocc: int, device: str | None = None) -> np.ndarray:
+    """D = 2 C C^T with C an M x nocc block with orthonormal columns.
+
+    With ``device`` (a torch device string) the QR and the product run there in
+    float64 -- the same matrices up to rounding, much faster for M ~ 16 000.
+    """
     nocc = min(nocc, M)
-    C, _ = np.linalg.qr(rng.standard_normal((M, nocc)))
+    G = rng.standard_normal((M, nocc))
+    if device is not None:
+        import torch
+        Ct, _ = torch.linalg.qr(torch.as_tensor(G, device=device))
+        Dt = 2.0 * (Ct @ Ct.T)
+        Dt = 0.5 * (Dt + Dt.T)
+        return Dt.cpu().numpy()
+    C, _ = np.linalg.qr(G)
     D = 2.0 * (C @ C.T)
     return 0.5 * (D + D.T)
 
@@ -171,7 +182,8 @@ def _ao_atom_index(shells: list[Shell]) -> np.ndarray:
 
 def make_molecule(config: str = "c1", seed: int = 0, natom: int | None = None,
                   box: float | None = None, nocc: int | None = None,
-                  generalised: bool = False, cutoff: float | None = None) -> SyntheticMolecule:
+                  generalised: bool = False, cutoff: float | None = None,
+                  device: str | None = None) -> SyntheticMolecule:
     """Build the synthetic molecule of one benchmark configuration.
 
     c1: 12 atoms in an 8 bohr box, Cartesian up to d, ~140 functions, 20 occupied.
@@ -198,11 +210,11 @@ def make_molecule(config: str = "c1", seed: int = 0, natom: int | None = None,
     numbers = rng.choice(np.array([1, 6, 8]), size=natom)
     shells = make_basis(rng, coords, numbers, RECIPES[config], generalised=generalised)
     M = sum(nfunc(a) for s in shells for a in s.angmoms)
-    D = make_density_matrix(rng, M, nocc)
+    D = make_density_matrix(rng, M, nocc, device=device)
     if cutoff is not None:
         at = _ao_atom_index(shells)
-        dist = np.linalg.norm(coords[at][:, None, :] - coords[at][None, :, :], axis=-1)
-        D[dist > cutoff] = 0.0
+        adist = np.linalg.norm(coords[:, None, :] - coords[None, :, :], axis=-1)
+        D[(adist > cutoff)[np.ix_(at, at)]] = 0.0
     return SyntheticMolecule(coords=coords, numbers=numbers.astype(np.int32),
                              charges=numbers.astype(np.float64), shells=shells, D=D,
                              name=config, meta=dict(seed=seed, box=box, nocc=nocc))

@@ -79,6 +79,18 @@ def test_tc_large_molecule_slice(torch_cuda):
     _check(mol, pts)
 
 
+@pytest.mark.parametrize("natom,seed", [(150, 0), (60, 5)])
+def test_tc_cartesian_g_cutoff_molecule(torch_cuda, natom, seed):
+    """Molecules of the 1000-atom generator at its density (Cartesian up to g,
+    D zeroed beyond 12 bohr), points within ~1 bohr of the atoms: AO rows with
+    one steep g function and many small entries, the case that needs the
+    fifth digit of the A operand (31-bit rows gave 2e-8 here)."""
+    mol = S.make_molecule("c4", seed=seed, natom=natom, box=(natom / 0.01) ** (1 / 3))
+    rng = np.random.default_rng(seed)
+    pts = mol.coords[rng.integers(0, len(mol.coords), 96)] + rng.normal(0, 1.0, (96, 3))
+    _check(mol, pts)
+
+
 def test_tc_matches_fp64_path_on_cube(torch_cuda):
     mol, _ = _cases().CASES["c1"]()
     m = ctc_abi.Mol(mol.flat(), mol.coords, mol.charges, mol.D)
