@@ -33,7 +33,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread",
               "--expt-relaxed-constexpr", "-I" + INCLUDE] + ARCH
 CU_SOURCES = ["ctc_basis.cu", "ctc_ao.cu", "ctc_local.cu", "ctc_tc.cu", "ctc_esp.cu",
-              "ctc_adjoint.cu", "ctc_api.cu", "ctc_noalloc.cu"]
+              "ctc_adjoint.cu", "ctc_api.cu", "ctc_noalloc.cu", "ctc_fchk.cpp"]
 HEADERS = ["ctc_internal.h", "ctc_terms.inc", "ctc_ao_poly.inc", "ctc_tiles.cuh", "ctc_split.cuh"]
 
 
@@ -58,7 +58,7 @@ def build(verbose: bool = False) -> str:
     objs = []
     for s in CU_SOURCES:
         src = os.path.join(CSRC, s)
-        obj = os.path.join(BUILD, s.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(s)[0] + ".o")
         objs.append(obj)
         if _newer([src] + hdrs, obj):
             jobs.append([NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj])

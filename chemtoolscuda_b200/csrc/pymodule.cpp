@@ -106,6 +106,31 @@ class Molecule {
     return std::make_unique<Molecule>(h, arr(coords), nums, path);
   }
 
+  // Molecule(path): a Gaussian formatted checkpoint file read by the library's
+  // native reader (the reference's Molecule(str), src/pybind.cpp:15, loads it
+  // through the Python iodata package).
+  static std::unique_ptr<Molecule> from_fchk(const std::string& path) {
+    ctc_fchk* f = nullptr;
+    check(ctc_fchk_load(path.c_str(), &f), "Molecule");
+    ctc_fchk_view v;
+    ctc_fchk_view_get(f, &v);
+    ctc_molecule* h = nullptr;
+    int rc;
+    {
+      py::gil_scoped_release rel;
+      rc = ctc_molecule_create(&v.basis, v.natom, v.atom_xyz, v.atom_charges, v.density, v.nbasis, &h);
+    }
+    arr coords({(py::ssize_t)v.natom, (py::ssize_t)3});
+    iarr nums((py::ssize_t)v.natom);
+    for (int a = 0; a < v.natom; ++a) {
+      for (int d = 0; d < 3; ++d) coords.mutable_data()[3 * a + d] = v.atom_xyz[3 * a + d];
+      nums.mutable_data()[a] = v.atomic_numbers[a];
+    }
+    ctc_fchk_destroy(f);
+    check(rc, "Molecule");
+    return std::make_unique<Molecule>(h, coords, nums, path);
+  }
+
   // ---- generic evaluation (host arrays) ----
   py::dict local(const arr& pts_in, const std::vector<std::string>& keys, const std::string& prec,
                  double alpha, double gge_a, double gge_b, double ked_a) {
@@ -265,6 +290,9 @@ PYBIND11_MODULE(_chemtools_cuda, m) {
   m.def("last_error", []() { return std::string(ctc_last_error()); });
 
   py::class_<Molecule>(m, "Molecule")
+      .def(py::init(&Molecule::from_fchk), py::arg("file_path"),
+           "Molecule from a Gaussian formatted checkpoint (.fchk) file.")
+      .def_static("from_fchk", &Molecule::from_fchk, py::arg("file_path"))
       .def_static("from_arrays", &Molecule::from_arrays, py::arg("centers"), py::arg("shell_atom"),
                   py::arg("nprim"), py::arg("nseg"), py::arg("angmoms"), py::arg("exps"),
                   py::arg("coeffs"), py::arg("coords"), py::arg("charges"), py::arg("D"),

@@ -108,6 +108,32 @@ int ctc_molecule_set_coordinates(ctc_molecule* mol, const double* atom_xyz);
  * Molecule::basis_set_to_constant_memory (src/pymolecule.cu:25-32). */
 int ctc_molecule_prepare(ctc_molecule* mol, int32_t precision);
 
+/* ---- Gaussian formatted checkpoint files ----------------------------------
+ * Replaces chemtools::get_molecular_basis_from_fchk (src/iodata.cpp:15-211),
+ * which reads the file through the Python iodata package, and the Molecule(str)
+ * constructor built on it (src/pymolecule.cu:18-23).  The density matrix is the
+ * MO one-particle density matrix (C occ) C^T as the reference forms it
+ * (src/iodata.cpp:157-160); basis functions keep Gaussian's order within each
+ * shell, which is the order of the reference's kernels. */
+typedef struct ctc_fchk ctc_fchk;
+
+typedef struct {
+  ctc_basis basis;              /* arrays owned by the ctc_fchk */
+  int32_t natom;
+  const double* atom_xyz;       /* [natom][3], bohr */
+  const double* atom_charges;   /* [natom] nuclear charges */
+  const int32_t* atomic_numbers;/* [natom] */
+  int32_t nbasis;
+  int32_t nalpha, nbeta;        /* electrons */
+  const double* density;        /* [nbasis][nbasis] */
+} ctc_fchk_view;
+
+int ctc_fchk_load(const char* path, ctc_fchk** out);
+int ctc_fchk_view_get(const ctc_fchk* f, ctc_fchk_view* out);
+void ctc_fchk_destroy(ctc_fchk* f);
+/* ctc_molecule_create with the contents of an .fchk file. */
+int ctc_molecule_create_from_fchk(const char* path, ctc_molecule** out);
+
 /* ---- local descriptors --------------------------------------------------------------------- */
 
 /* All requested local descriptors at N points in one fused pass.  Replaces

@@ -28,6 +28,12 @@ class Basis(C.Structure):
                 ("exps", C.c_void_p), ("coeffs", C.c_void_p)]
 
 
+class FchkView(C.Structure):
+    _fields_ = [("basis", Basis), ("natom", C.c_int32), ("atom_xyz", C.c_void_p),
+                ("atom_charges", C.c_void_p), ("atomic_numbers", C.c_void_p), ("nbasis", C.c_int32),
+                ("nalpha", C.c_int32), ("nbeta", C.c_int32), ("density", C.c_void_p)]
+
+
 class Outputs(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in OUT_KEYS]
 
@@ -67,7 +73,41 @@ def lib():
         L.ctc_eval_esp.argtypes = [vp, vp, i64, vp, vp]
         L.ctc_eval_esp_host.argtypes = [vp, vp, i64, vp]
         L.ctc_adjoint.argtypes = [vp, vp, i64, vp, vp, vp, vp, vp]
+        L.ctc_fchk_load.argtypes = [C.c_char_p, vp]
+        L.ctc_fchk_view_get.argtypes = [vp, vp]
+        L.ctc_fchk_destroy.argtypes = [vp]
+        L.ctc_fchk_destroy.restype = None
+        L.ctc_molecule_create_from_fchk.argtypes = [C.c_char_p, vp]
     return _lib
+
+
+def load_fchk(path: str) -> dict:
+    """Basis (flat layout of synthetic.flatten_basis), atoms and density matrix of an .fchk
+    file as read by the library's native reader (host only, no GPU needed)."""
+    h = C.c_void_p()
+    check(lib().ctc_fchk_load(path.encode(), C.byref(h)), "ctc_fchk_load")
+    try:
+        v = FchkView()
+        check(lib().ctc_fchk_view_get(h, C.byref(v)), "ctc_fchk_view_get")
+        b = v.basis
+        ns = b.nshell
+
+        def arr(ptr, n, ct):
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,)).copy()
+        nprim = arr(b.nprim, ns, C.c_int32)
+        nseg = arr(b.nseg, ns, C.c_int32)
+        flat = dict(centers=arr(b.centers, 3 * ns, C.c_double).reshape(ns, 3),
+                    shell_atom=arr(b.shell_atom, ns, C.c_int32), nprim=nprim, nseg=nseg,
+                    angmoms=arr(b.angmoms, int(nseg.sum()), C.c_int32),
+                    exps=arr(b.exps, int(nprim.sum()), C.c_double),
+                    coeffs=arr(b.coeffs, int((nseg * nprim).sum()), C.c_double))
+        M = v.nbasis
+        return dict(flat=flat, coords=arr(v.atom_xyz, 3 * v.natom, C.c_double).reshape(v.natom, 3),
+                    charges=arr(v.atom_charges, v.natom, C.c_double),
+                    numbers=arr(v.atomic_numbers, v.natom, C.c_int32), nalpha=v.nalpha, nbeta=v.nbeta,
+                    D=arr(v.density, M * M, C.c_double).reshape(M, M))
+    finally:
+        lib().ctc_fchk_destroy(h)
 
 
 def err() -> str:
