@@ -652,7 +652,7 @@ def run_workload(args):
         err = _sample_errors({k: got[k][idx] for k in keys}, ref, sc, keys)
         line.update({"metric": "grid pts/s for rho, grad rho, lap rho (1000-atom molecule, tensor-core path)",
                      "value": n / (ms * 1e-3), "unit": "grid points/s", "ms_per_step": ms,
-                     "higher_is_better": True, "dtype": "int8x4 split operands, exact int32 accumulation, fp64 AO/epilogue",
+                     "higher_is_better": True, "dtype": "int8 digit split (5 AO x 4 D digits), exact int32 accumulation, fp64 AO/epilogue",
                      "config": {"workload": "c4: 1000 atoms, Cartesian up to g, D zeroed beyond 12 bohr, 368^3 cube at 0.25 bohr",
                                 "nbasis": mol.nbasis, "points": n,
                                 "mean_compact_aos_per_tile": st[2] / max(st[0], 1)},
@@ -722,7 +722,7 @@ def main():
         return 0
     res, fp64, e2e, esp, cpu, nbasis = run_ours(args, ws, rank, local)
     if rank == 0:
-        dtype = ("int8x4 split operands, exact int32 accumulation, fp64 AO/epilogue"
+        dtype = ("int8 digit split (5 AO x 4 D digits), exact int32 accumulation, fp64 AO/epilogue"
                  if args.precision == "tc" else "f64")
         line = {
             "metric": METRIC, "value": res["value"], "unit": "grid points/s", "n_gpus": ws,

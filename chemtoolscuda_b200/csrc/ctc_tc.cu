@@ -510,8 +510,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     }
   } else if (warp == 4) {
     // ---------------- MMA issuer
-    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
-                           ((uint32_t)(kRows >> 4) << 24);
+    // One MMA per A digit plane pa and K step: B is the stage's four D planes
+    // read as one operand of 64 * nb rows (the planes are contiguous), so the
+    // MMA's column block j is the product a_pa b_j and lands at TMEM column
+    // (pa + j) * 64, the accumulator of level L = pa + j.  nb = min(4, 5 - pa)
+    // keeps L <= 4.  At the first K step of a nu tile pa = 0 (levels 0-3) and
+    // pa = 4 (level 4) initialise the 320 columns; every later MMA
+    // accumulates.  Five MMAs of N = 256, 256, 192, 128, 64 replace the 14
+    // N = 64 products: the same work in fewer, wider instructions.
+    const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRows >> 4) << 24);
     int it = 0, gnt = 0;  // stage and nu-tile counters across tiles
     for (int i = 0;; ++i) {
       const int t = read_tile(i);
@@ -526,7 +533,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         if (!mbar_wait(&tempty_bar, (gnt & 1) ^ 1)) { s_abort = 1; break; }
         tr1 += clock64() - tw;
         tc_fence_after();
-        uint32_t started = 0;  // bit L: level L accumulator initialised
         for (int kb = 0; kb < nkb; ++kb, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
@@ -539,18 +545,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
             const uint32_t b0 = smem_u32(sB + s * kBStageBytes);
 #pragma unroll
             for (int ks = 0; ks < kBK / 32; ++ks) {
+              const uint64_t bd = umma_desc_sw64(b0 + ks * 32);
+              const bool first = kb == 0 && ks == 0;
 #pragma unroll
-              for (int pa = 0; pa < kPlanesA; ++pa) {
-#pragma unroll
-                for (int pb = 0; pb < kPlanes; ++pb) {
-                  const int L = pa + pb;
-                  if (L >= kLevels) continue;
-                  const uint64_t ad = umma_desc_sw64(a0 + pa * kAPlaneBytes + ks * 32);
-                  const uint64_t bd = umma_desc_sw64(b0 + pb * kBPlaneBytes + ks * 32);
-                  const uint32_t acc = (started >> L) & 1u;
-                  umma_i8(tmem + L * kN, ad, bd, idesc, acc);
-                  started |= 1u << L;
-                }
+              for (int o = 0; o < kPlanesA; ++o) {
+                const int pa = o == 0 ? 0 : (o == 1 ? kPlanesA - 1 : o - 1);  // 0, 4, 1, 2, 3
+                const int nb = kPlanes < kLevels - pa ? kPlanes : kLevels - pa;
+                const uint32_t idesc = idesc0 | ((uint32_t)(nb * kN >> 3) << 17);
+                const uint64_t ad = umma_desc_sw64(a0 + pa * kAPlaneBytes + ks * 32);
+                umma_i8(tmem + pa * kN, ad, bd, idesc, (first && o < 2) ? 0u : 1u);
               }
             }
             umma_commit(&empty_bar[s]);

@@ -1,4 +1,4 @@
-"""GPU parity of the tensor-core split path (INT8 tcgen05, 4-way split
+"""GPU parity of the tensor-core split path (INT8 tcgen05, 5-digit AO and 4-digit D
 operands, exact int32 accumulation) against the FP64 oracle.
 
 Stated tolerance: 1e-8 relative to the per-point sum of absolute terms
