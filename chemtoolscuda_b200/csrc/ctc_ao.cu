@@ -264,15 +264,16 @@ __global__ void __launch_bounds__(kAoThreads, 3)
 }
 
 // Digit planes of the tile rows (ctc_split.cuh) with the exponents found by
-// ao_tile_kernel.  Block (t, y) covers K columns [256 y, 256 y + 256) of tile
-// t, so a tile's work spreads over K / 256 blocks.  Work items are (32-row
-// group, 32-column chunk): a warp reads one 256-byte line per column (32
-// consecutive rows = points of one quantity) and each lane writes 32 bytes per
-// plane of its own row.
+// ao_tile_kernel.  Block (t, y) covers K columns [64 y, 64 y + 64) of tile t,
+// so a tile's work spreads over K / 64 blocks.  Work items are (32-row group,
+// 32-column chunk), one per warp: a warp reads one 256-byte line per column
+// (32 consecutive rows = points of one quantity), all 32 lines before any
+// conversion so that they are in flight together, and each lane writes 32
+// bytes per plane of its own row.
 constexpr int kSliceThreads = 256;
-constexpr int kSliceCols = 256;
+constexpr int kSliceCols = 64;
 
-__global__ void __launch_bounds__(kSliceThreads)
+__global__ void __launch_bounds__(kSliceThreads, 2)
     slice_rows_kernel(TileBatch tb, int nqa, const int32_t* __restrict__ eexp,
                       int8_t* __restrict__ planes) {
   const int t = blockIdx.x;
@@ -293,7 +294,10 @@ __global__ void __launch_bounds__(kSliceThreads)
     const int p = nqa == 4 ? lane : r;
     const double f = split_row_factor(eexp[(int64_t)t * kSplitRows + r], kFixedBitsA);
     const double* col = A + q * ld_q + p + (int64_t)(c * 32) * TP;
-    write_row_digits32([&](int i) { return __ldg(col + (int64_t)i * TP); }, f, P, r, tb.Kcap, c * 32);
+    double v[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __ldg(col + (int64_t)i * TP);
+    write_row_digits32([&](int i) { return v[i]; }, f, P, r, tb.Kcap, c * 32);
   }
 }
 

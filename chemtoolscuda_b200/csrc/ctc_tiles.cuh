@@ -92,6 +92,7 @@ __device__ __forceinline__ void finalize_point(const double* s, int nqa, int nq_
 
 // ------------------------------------------------------------------ tiles
 constexpr int kTileThreads = 256;
+constexpr int kSortCap = 2048;  // segment lists up to this length are ordered by type
 
 __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   v &= 0x3ffu;
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(kTileThreads)
                   double* __restrict__ stats) {
   using Scan = cub::BlockScan<int, kTileThreads>;
   __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ int s_sl[kSortCap], s_k0[kSortCap], s_cnt[8];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ double sctr[3], srad;
   __shared__ int base_s, base_k;
@@ -230,6 +232,37 @@ __global__ void __launch_bounds__(kTileThreads)
       base_k += tot.y;
     }
     __syncthreads();
+  }
+  // Visit order for the AO kernel: the significant segments grouped by type
+  // (counting sort; compact positions k0 keep the AO order), so that the
+  // warps of a CTA run one type's evaluation code at a time instead of
+  // alternating between the types' large unrolled bodies.
+  const int ns = base_s;
+  if (ns <= kSortCap) {
+    if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kTileThreads) {
+      const int sg = sl[i];
+      s_sl[i] = sg;
+      s_k0[i] = k0[i];
+      atomicAdd(&s_cnt[segs[sg].type & 7], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int ty = 0; ty < 8; ++ty) {
+        const int c = s_cnt[ty];
+        s_cnt[ty] = acc;
+        acc += c;
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ns; i += kTileThreads) {
+      const int sg = s_sl[i];
+      const int pos = atomicAdd(&s_cnt[segs[sg].type & 7], 1);
+      sl[pos] = sg;
+      k0[pos] = s_k0[i];
+    }
   }
   const int kt_true = base_k;
   const int kt = (kt_true + kKtAlign - 1) / kKtAlign * kKtAlign;
