@@ -216,10 +216,11 @@ __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __
 template <int DERIV, int SLICE>
 __global__ void __launch_bounds__(kAoThreads, 3)
     ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
-                   const double* __restrict__ coef, TileBatch tb, int32_t* __restrict__ eexp) {
+                   const double* __restrict__ coef, TileBatch tb, int32_t* __restrict__ eexp,
+                   const int32_t* __restrict__ order) {
   // per-warp maxima of the high word of |value| per row, [warp][row]
   __shared__ unsigned s_mx[SLICE ? kAoThreads / 32 : 1][SLICE ? kSplitRows : 1];
-  const int t = blockIdx.x;
+  const int t = order ? order[blockIdx.x] : blockIdx.x;
   const int ns = tb.nsig[t], TP = tb.TP;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t* sl = tb.segs + (int64_t)t * nseg;
@@ -341,16 +342,16 @@ int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cud
   if (tb.C <= 0) return CTC_OK;
   const auto* sg = mol->d_segs;
   switch (deriv) {
-    case 0: ao_tile_kernel<0, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr); break;
-    case 1: ao_tile_kernel<1, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr); break;
-    default: ao_tile_kernel<2, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr);
+    case 0: ao_tile_kernel<0, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr, nullptr); break;
+    case 1: ao_tile_kernel<1, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr, nullptr); break;
+    default: ao_tile_kernel<2, 0><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, mol->d_alpha, mol->d_coef, tb, nullptr, nullptr);
   }
   CTC_CUDA_TRY(cudaGetLastError());
   return CTC_OK;
 }
 
 int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
-                           int8_t* planes, int32_t* eexp, cudaStream_t st) {
+                           int8_t* planes, int32_t* eexp, const int32_t* order, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
   if (!(nqa == 4 && tb.TP == 32 && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
     return fail(CTC_ERR_INVALID, "sliced AO tiles: unsupported row layout");
@@ -359,13 +360,13 @@ int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int der
   const auto* sg = mol->d_segs;
   const double *al = mol->d_alpha, *co = mol->d_coef;
   if (nqa == 4) {
-    if (deriv == 1) ao_tile_kernel<1, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
-    else ao_tile_kernel<2, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
+    if (deriv == 1) ao_tile_kernel<1, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp, order);
+    else ao_tile_kernel<2, 4><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp, order);
   } else {
     switch (deriv) {
-      case 0: ao_tile_kernel<0, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp); break;
-      case 1: ao_tile_kernel<1, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp); break;
-      default: ao_tile_kernel<2, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp);
+      case 0: ao_tile_kernel<0, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp, order); break;
+      case 1: ao_tile_kernel<1, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp, order); break;
+      default: ao_tile_kernel<2, 1><<<tb.C, kAoThreads, 0, st>>>(sg, mol->nseg, al, co, tb, eexp, order);
     }
   }
   CTC_CUDA_TRY(cudaGetLastError());

@@ -156,8 +156,9 @@ int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cud
 // (nqa = 4: 32 points x {phi, d phi}; nqa = 1: 128 points x phi) with one
 // exponent per row, for the tensor-core split path: planes [C][5][128][Kcap],
 // eexp [C][128].
+// order (optional) lists the tiles in the order the CTAs take them.
 int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
-                           int8_t* planes, int32_t* eexp, cudaStream_t st);
+                           int8_t* planes, int32_t* eexp, const int32_t* order, cudaStream_t st);
 int launch_ao(const ctc_molecule* mol, const PointSrc& src, int64_t n, int deriv, double* out,
               int nq_out, int ld, cudaStream_t st);
 // AO output in (nq, n, M) layout for ctc_eval_ao.
@@ -176,9 +177,11 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
 
 // ---- tensor-core split path (ctc_tc.cu) ----
 int prepare_tc(ctc_molecule* mol, cudaStream_t st);
-// Workspace of the digit planes and row exponents of a chunk of tiles.
+// Workspace of the digit planes and row exponents of a chunk of tiles, and
+// the chunk's tile order (largest compact K first), computed here from tb.kt;
+// tc_local_tiles on the same batch uses all three.
 int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
-                       int32_t** eexp);
+                       int32_t** eexp, const int32_t** order);
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
 

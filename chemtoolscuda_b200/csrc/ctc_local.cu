@@ -80,9 +80,10 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
   const std::function<int(const TileBatch&)> sliced_ao = [&](const TileBatch& tb) {
     int8_t* planes = nullptr;
     int32_t* eexp = nullptr;
-    int r = tc_slice_workspace(mol, tb, st, &planes, &eexp);
+    const int32_t* order = nullptr;
+    int r = tc_slice_workspace(mol, tb, st, &planes, &eexp, &order);
     if (r != CTC_OK) return r;
-    return launch_ao_tiles_sliced(mol, tb, plan.deriv, plan.nqa, planes, eexp, st);
+    return launch_ao_tiles_sliced(mol, tb, plan.deriv, plan.nqa, planes, eexp, order, st);
   };
   int rc = run_tiles(
       mol, src, n, TP, plan.nq_ao, plan.deriv, st,

@@ -843,16 +843,6 @@ int tc_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, TcWork
   return CTC_OK;
 }
 
-int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
-                       int32_t** eexp) {
-  TcWorkspace w;
-  const int rc = tc_workspace(mol, tb, st, &w);
-  if (rc != CTC_OK) return rc;
-  *planes = w.planes;
-  *eexp = w.eexp;
-  return CTC_OK;
-}
-
 namespace {
 // sort keys: largest compact K first (ascending kMaxKt - kt), ids = tile index
 __global__ void tile_order_keys_kernel(const int32_t* __restrict__ kt, int C, uint32_t* keys,
@@ -866,6 +856,24 @@ __global__ void tile_order_keys_kernel(const int32_t* __restrict__ kt, int C, ui
 }
 }  // namespace
 
+int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
+                       int32_t** eexp, const int32_t** order) {
+  TcWorkspace w;
+  const int rc = tc_workspace(mol, tb, st, &w);
+  if (rc != CTC_OK) return rc;
+  // the chunk's tile order, largest compact K first: the AO kernel's CTAs and
+  // the contraction's persistent CTAs both take the tiles in this order, so
+  // the last tiles of either launch are the cheapest ones
+  tile_order_keys_kernel<<<(tb.C + 255) / 256, 256, 0, st>>>(tb.kt, tb.C, w.keys_in, w.ids, w.counter);
+  CTC_CUDA_TRY(cudaGetLastError());
+  CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.keys_in, w.keys_out, w.ids,
+                                               w.order, tb.C, 0, 15, st));
+  *planes = w.planes;
+  *eexp = w.eexp;
+  *order = w.order;
+  return CTC_OK;
+}
+
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
@@ -873,16 +881,11 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
     return fail(CTC_ERR_UNSUPPORTED, "tensor-core split path: more than 16384 functions per tile");
   int rc = prepare_tc(mol, st);
   if (rc != CTC_OK) return rc;
-  // int8 planes of the tile rows + row exponents, written by this chunk's AO
-  // kernel (launch_ao_tiles_sliced)
+  // int8 planes of the tile rows, row exponents and the tile order (largest
+  // compact K first, zeroed tile counter), written for this chunk by
+  // tc_slice_workspace and the AO kernel (launch_ao_tiles_sliced)
   TcWorkspace w;
   if ((rc = tc_workspace(mol, tb, st, &w)) != CTC_OK) return rc;
-  // persistent CTAs take the chunk's tiles largest first, so the last tiles
-  // handed out are the cheapest ones
-  tile_order_keys_kernel<<<(tb.C + 255) / 256, 256, 0, st>>>(tb.kt, tb.C, w.keys_in, w.ids, w.counter);
-  CTC_CUDA_TRY(cudaGetLastError());
-  CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(w.sort_tmp, w.sort_bytes, w.keys_in, w.keys_out, w.ids,
-                                               w.order, tb.C, 0, 15, st));
   // tensor map over the planes: 2-D, rows = C*4*128, inner = Kcap bytes
   PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode();
   if (!enc) return fail(CTC_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
