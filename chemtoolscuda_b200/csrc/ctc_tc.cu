@@ -252,39 +252,47 @@ __device__ __forceinline__ constexpr int role_sum(int role, int slot, int row) {
 // the role's i-th sum (slot-major, rows in order).  G is the FP64 copy in
 // shared memory, [column][row]; ao points at AO quantity 0, column 0 of the nu
 // tile for this thread's point (element (q, c) at ao[q * ldq + c * 32]).
-template <int ROLE>
+// AO columns per load group of the epilogue contraction: 16 / GW register
+// buffers keep 16 - GW columns of AO values in flight per thread while one
+// group is reduced (measured: GW = 2 beats 4 and 8 on the 215^3 cube, the
+// loads being latency-bound on tiles with few columns)
+constexpr int kEpiGroup = 2;
+
+template <int ROLE, int GW>
 __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int64_t ldq,
                                               const double* __restrict__ sG, int lane, int nq_ao,
                                               uint64_t stream, double* acc) {
   constexpr int NS = role_nslot(ROLE);
-  constexpr int NG = kN / 8;  // groups of 8 columns
+  constexpr int NG = kN / GW;    // groups of GW columns
+  constexpr int NB = 16 / GW;    // register buffers of one group each
   bool live[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) live[s] = role_q(ROLE, s) < nq_ao;
-  // two register buffers: the loads of group g + 1 are in flight while group g
-  // is reduced
-  double a[2][NS][8];
+  // NB register buffers: the loads of groups g + 1 .. g + NB - 1 are in flight
+  // while group g is reduced
+  double a[NB][NS][GW];
   auto load = [&](int buf, int cg) {
 #pragma unroll
     for (int s = 0; s < NS; ++s)
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < GW; ++j)
         a[buf][s][j] = live[s] ? ldg_f64_stream(ao + role_q(ROLE, s) * ldq + (cg + j) * 32, stream) : 0.0;
   };
-  load(0, 0);
+#pragma unroll
+  for (int g = 0; g < NB - 1; ++g) load(g, g * GW);
 #pragma unroll
   for (int g = 0; g < NG; ++g) {
-    if (g + 1 < NG) load((g + 1) & 1, (g + 1) * 8);
-    const int cg = g * 8;
+    if (g + NB - 1 < NG) load((g + NB - 1) % NB, (g + NB - 1) * GW);
+    const int cg = g * GW;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < GW; ++j) {
       const double* gp = sG + (cg + j) * kRows + lane;
       int i = 0;
 #pragma unroll
       for (int s = 0; s < NS; ++s)
 #pragma unroll
         for (int rr = 0; rr < role_nrow(ROLE, s); ++rr, ++i)
-          acc[i] = fma(gp[rr * 32], a[g & 1][s][j], acc[i]);
+          acc[i] = fma(gp[rr * 32], a[g % NB][s][j], acc[i]);
     }
   }
 }
@@ -655,10 +663,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         const double* ao_nt = aop + (int64_t)n0 * PTS;
         if (NQA == 4) {
           switch (role) {
-            case 0: contract_role<0>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-            case 1: contract_role<1>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-            case 2: contract_role<2>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
-            default: contract_role<3>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            case 0: contract_role<0, kEpiGroup>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            case 1: contract_role<1, kEpiGroup>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            case 2: contract_role<2, kEpiGroup>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
+            default: contract_role<3, kEpiGroup>(ao_nt, ldq, sG, lane, nq_ao, stream, acc); break;
           }
         } else {
           // rows are points: sums over the nq_ao (1 or 4) quantities of this point
