@@ -265,31 +265,27 @@ __global__ void __launch_bounds__(kAoThreads, 3)
 }
 
 // Digit planes of the tile rows (ctc_split.cuh) with the exponents found by
-// ao_tile_kernel.  Block (t, y) covers K columns [64 y, 64 y + 64) of tile t,
-// so a tile's work spreads over K / 64 blocks.  Work items are (32-row group,
-// 32-column chunk), one per warp: a warp reads one 256-byte line per column
-// (32 consecutive rows = points of one quantity), all 32 lines before any
-// conversion so that they are in flight together, and each lane writes 32
-// bytes per plane of its own row.
+// ao_tile_kernel.  One block per tile, the tiles taken in the chunk's order
+// (largest compact K first) when one is given.  Work items are (32-row
+// group, 32-column chunk); the block's warps take them in turn: a warp reads
+// one 256-byte line per column (32 consecutive rows = points of one
+// quantity), all 32 lines before any conversion so that they are in flight
+// together, and each lane writes 32 bytes per plane of its own row.
 constexpr int kSliceThreads = 256;
-constexpr int kSliceCols = 64;
 
 __global__ void __launch_bounds__(kSliceThreads, 2)
     slice_rows_kernel(TileBatch tb, int nqa, const int32_t* __restrict__ eexp,
-                      int8_t* __restrict__ planes) {
-  const int t = blockIdx.x;
+                      int8_t* __restrict__ planes, const int32_t* __restrict__ order) {
+  const int t = order ? order[blockIdx.x] : blockIdx.x;
   const int kt = tb.kt[t];
-  const int kbeg = blockIdx.y * kSliceCols;
-  if (kbeg >= kt) return;
   const int TP = tb.TP;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t ld_q = (int64_t)TP * tb.Kcap;
   const double* A = tb.ao + (int64_t)t * tb.nq * ld_q;
   int8_t* P = planes + (int64_t)t * kSplitPlanesA * kSplitRows * tb.Kcap;
-  const int nchunk = min(kt - kbeg, kSliceCols) / 32;
-  const int nitem = (kSplitRows / 32) * nchunk;  // warp-sized items
+  const int nitem = (kSplitRows / 32) * (kt / 32);  // warp-sized items
   for (int it = warp; it < nitem; it += kSliceThreads / 32) {
-    const int rg = it % (kSplitRows / 32), c = kbeg / 32 + it / (kSplitRows / 32);
+    const int rg = it % (kSplitRows / 32), c = it / (kSplitRows / 32);
     const int r = rg * 32 + lane;
     const int q = nqa == 4 ? rg : 0;
     const int p = nqa == 4 ? lane : r;
@@ -370,8 +366,7 @@ int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int der
     }
   }
   CTC_CUDA_TRY(cudaGetLastError());
-  const dim3 sgrid((unsigned)tb.C, (unsigned)((tb.Kcap + kSliceCols - 1) / kSliceCols));
-  slice_rows_kernel<<<sgrid, kSliceThreads, 0, st>>>(tb, nqa, eexp, planes);
+  slice_rows_kernel<<<tb.C, kSliceThreads, 0, st>>>(tb, nqa, eexp, planes, order);
   CTC_CUDA_TRY(cudaGetLastError());
   return CTC_OK;
 }
