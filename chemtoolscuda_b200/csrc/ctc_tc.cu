@@ -254,8 +254,9 @@ __device__ __forceinline__ constexpr int role_sum(int role, int slot, int row) {
 // tile for this thread's point (element (q, c) at ao[q * ldq + c * 32]).
 // AO columns per load group of the epilogue contraction: 16 / GW register
 // buffers keep 16 - GW columns of AO values in flight per thread while one
-// group is reduced (measured: GW = 2 beats 4 and 8 on the 215^3 cube, the
-// loads being latency-bound on tiles with few columns)
+// group is reduced (measured on the 215^3 cube: GW = 2 beats 8 (335 -> 317 ms),
+// 4 (328 ms) and 1 (318 ms); the loads are latency-bound on tiles with few
+// columns)
 constexpr int kEpiGroup = 2;
 
 template <int ROLE, int GW>
