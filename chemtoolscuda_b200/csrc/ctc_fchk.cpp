@@ -31,19 +31,10 @@
 #include <vector>
 
 #include "ctc_internal.h"
+#include "ctc_wfnfile.h"
 
 using namespace ctc;
 
-struct ctc_fchk {
-  std::string path;
-  int32_t natom = 0, nbasis = 0, nalpha = 0, nbeta = 0;
-  std::vector<int32_t> numbers;
-  std::vector<double> charges, coords;
-  // ctc_basis arrays
-  std::vector<double> centers, exps, coeffs;
-  std::vector<int32_t> shell_atom, nprim, nseg, angmoms;
-  std::vector<double> D;  // nbasis x nbasis, row-major (symmetric)
-};
 
 namespace {
 

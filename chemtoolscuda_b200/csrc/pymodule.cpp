@@ -7,6 +7,7 @@
 // and basis_set_to_constant_memory.  Points are numpy (N, 3) float64 arrays;
 // results come back as fresh numpy arrays of the reference's shapes.  All work
 // goes through the C ABI of include/chemtools_cuda.h with the GIL released.
+#include <cctype>
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -106,12 +107,21 @@ class Molecule {
     return std::make_unique<Molecule>(h, arr(coords), nums, path);
   }
 
-  // Molecule(path): a Gaussian formatted checkpoint file read by the library's
-  // native reader (the reference's Molecule(str), src/pybind.cpp:15, loads it
-  // through the Python iodata package).
+  // Molecule(path): a Gaussian formatted checkpoint file, or a Molden file
+  // (.molden, .molden.input, .mold), read by the library's native readers
+  // (the reference's Molecule(str), src/pybind.cpp:15, loads either through
+  // the Python iodata package).
+  static bool is_molden(std::string p) {
+    for (char& c : p) c = (char)std::tolower((unsigned char)c);
+    for (const char* e : {".molden", ".molden.input", ".mold"}) {
+      const std::string s(e);
+      if (p.size() >= s.size() && p.compare(p.size() - s.size(), s.size(), s) == 0) return true;
+    }
+    return false;
+  }
   static std::unique_ptr<Molecule> from_fchk(const std::string& path) {
     ctc_fchk* f = nullptr;
-    check(ctc_fchk_load(path.c_str(), &f), "Molecule");
+    check(is_molden(path) ? ctc_molden_load(path.c_str(), &f) : ctc_fchk_load(path.c_str(), &f), "Molecule");
     ctc_fchk_view v;
     ctc_fchk_view_get(f, &v);
     ctc_molecule* h = nullptr;
@@ -291,7 +301,7 @@ PYBIND11_MODULE(_chemtools_cuda, m) {
 
   py::class_<Molecule>(m, "Molecule")
       .def(py::init(&Molecule::from_fchk), py::arg("file_path"),
-           "Molecule from a Gaussian formatted checkpoint (.fchk) file.")
+           "Molecule from a Gaussian formatted checkpoint (.fchk) or Molden (.molden) file.")
       .def_static("from_fchk", &Molecule::from_fchk, py::arg("file_path"))
       .def_static("from_arrays", &Molecule::from_arrays, py::arg("centers"), py::arg("shell_atom"),
                   py::arg("nprim"), py::arg("nseg"), py::arg("angmoms"), py::arg("exps"),

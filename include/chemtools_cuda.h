@@ -134,6 +134,20 @@ void ctc_fchk_destroy(ctc_fchk* f);
 /* ctc_molecule_create with the contents of an .fchk file. */
 int ctc_molecule_create_from_fchk(const char* path, ctc_molecule** out);
 
+/* ---- Molden files -----------------------------------------------------------
+ * The other wavefunction format the reference's Molecule(str) accepts through
+ * iodata (src/pymolecule.cu:18-23, src/iodata.cpp:15-211).  Fills the same
+ * ctc_fchk handle as ctc_fchk_load (read it with ctc_fchk_view_get, release it
+ * with ctc_fchk_destroy): atoms, [GTO] shells with the [5D]/[5D10F]/[7F]/
+ * [5D7F]/[9G] spherical flags, basis functions in the library's order
+ * (Molden's Cartesian g order is permuted), and the density matrix
+ * sum_i occ_i c_i c_i^T over the [MO] orbitals with their occupations. */
+int ctc_molden_load(const char* path, ctc_fchk** out);
+/* ctc_molecule_create from a wavefunction file, by extension: .molden,
+ * .molden.input and .mold are read as Molden files, anything else as fchk.
+ * Replaces Molecule(str) (src/pymolecule.cu:18-23). */
+int ctc_molecule_create_from_file(const char* path, ctc_molecule** out);
+
 /* ---- local descriptors --------------------------------------------------------------------- */
 
 /* All requested local descriptors at N points in one fused pass.  Replaces

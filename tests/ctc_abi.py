@@ -78,14 +78,20 @@ def lib():
         L.ctc_fchk_destroy.argtypes = [vp]
         L.ctc_fchk_destroy.restype = None
         L.ctc_molecule_create_from_fchk.argtypes = [C.c_char_p, vp]
+        L.ctc_molden_load.argtypes = [C.c_char_p, vp]
+        L.ctc_molecule_create_from_file.argtypes = [C.c_char_p, vp]
     return _lib
 
 
-def load_fchk(path: str) -> dict:
+def load_fchk(path: str, molden: bool = False) -> dict:
     """Basis (flat layout of synthetic.flatten_basis), atoms and density matrix of an .fchk
-    file as read by the library's native reader (host only, no GPU needed)."""
+    (or, with molden=True, a Molden) file as read by the library's native reader (host only,
+    no GPU needed)."""
     h = C.c_void_p()
-    check(lib().ctc_fchk_load(path.encode(), C.byref(h)), "ctc_fchk_load")
+    if molden:
+        check(lib().ctc_molden_load(path.encode(), C.byref(h)), "ctc_molden_load")
+    else:
+        check(lib().ctc_fchk_load(path.encode(), C.byref(h)), "ctc_fchk_load")
     try:
         v = FchkView()
         check(lib().ctc_fchk_view_get(h, C.byref(v)), "ctc_fchk_view_get")
@@ -108,6 +114,10 @@ def load_fchk(path: str) -> dict:
                     D=arr(v.density, M * M, C.c_double).reshape(M, M))
     finally:
         lib().ctc_fchk_destroy(h)
+
+
+def load_molden(path: str) -> dict:
+    return load_fchk(path, molden=True)
 
 
 def err() -> str:
