@@ -34,7 +34,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
               "--expt-relaxed-constexpr", "-I" + INCLUDE] + ARCH
 CU_SOURCES = ["ctc_basis.cu", "ctc_ao.cu", "ctc_local.cu", "ctc_tc.cu", "ctc_esp.cu",
               "ctc_adjoint.cu", "ctc_api.cu", "ctc_noalloc.cu", "ctc_fchk.cpp",
-              "ctc_molden.cpp"]
+              "ctc_molden.cpp", "ctc_wfn.cpp"]
 HEADERS = ["ctc_internal.h", "ctc_terms.inc", "ctc_ao_poly.inc", "ctc_tiles.cuh", "ctc_split.cuh",
            "ctc_wfnfile.h"]
 

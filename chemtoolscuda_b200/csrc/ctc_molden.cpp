@@ -313,8 +313,9 @@ int ctc_molecule_create_from_file(const char* path, ctc_molecule** out) {
   const std::string p = lower(path);
   auto ends = [&](const std::string& s) { return p.size() >= s.size() && p.compare(p.size() - s.size(), s.size(), s) == 0; };
   const bool molden = ends(".molden") || ends(".molden.input") || ends(".mold");
+  const bool wfn = ends(".wfn") || ends(".wfx");
   ctc_fchk* f = nullptr;
-  int rc = molden ? ctc_molden_load(path, &f) : ctc_fchk_load(path, &f);
+  int rc = molden ? ctc_molden_load(path, &f) : wfn ? ctc_wfn_load(path, &f) : ctc_fchk_load(path, &f);
   if (rc != CTC_OK) return rc;
   ctc_fchk_view v;
   ctc_fchk_view_get(f, &v);

@@ -13,6 +13,7 @@
 #include <pybind11/stl.h>
 
 #include <cstdint>
+#include <initializer_list>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -107,13 +108,13 @@ class Molecule {
     return std::make_unique<Molecule>(h, arr(coords), nums, path);
   }
 
-  // Molecule(path): a Gaussian formatted checkpoint file, or a Molden file
-  // (.molden, .molden.input, .mold), read by the library's native readers
-  // (the reference's Molecule(str), src/pybind.cpp:15, loads either through
-  // the Python iodata package).
-  static bool is_molden(std::string p) {
+  // Molecule(path): a Gaussian formatted checkpoint file, a Molden file
+  // (.molden, .molden.input, .mold) or an AIM wavefunction file (.wfn, .wfx),
+  // read by the library's native readers (the reference's Molecule(str),
+  // src/pybind.cpp:15, loads them through the Python iodata package).
+  static bool has_ext(std::string p, std::initializer_list<const char*> exts) {
     for (char& c : p) c = (char)std::tolower((unsigned char)c);
-    for (const char* e : {".molden", ".molden.input", ".mold"}) {
+    for (const char* e : exts) {
       const std::string s(e);
       if (p.size() >= s.size() && p.compare(p.size() - s.size(), s.size(), s) == 0) return true;
     }
@@ -121,7 +122,10 @@ class Molecule {
   }
   static std::unique_ptr<Molecule> from_fchk(const std::string& path) {
     ctc_fchk* f = nullptr;
-    check(is_molden(path) ? ctc_molden_load(path.c_str(), &f) : ctc_fchk_load(path.c_str(), &f), "Molecule");
+    check(has_ext(path, {".molden", ".molden.input", ".mold"}) ? ctc_molden_load(path.c_str(), &f)
+          : has_ext(path, {".wfn", ".wfx"})                     ? ctc_wfn_load(path.c_str(), &f)
+                                                                : ctc_fchk_load(path.c_str(), &f),
+          "Molecule");
     ctc_fchk_view v;
     ctc_fchk_view_get(f, &v);
     ctc_molecule* h = nullptr;
@@ -301,7 +305,7 @@ PYBIND11_MODULE(_chemtools_cuda, m) {
 
   py::class_<Molecule>(m, "Molecule")
       .def(py::init(&Molecule::from_fchk), py::arg("file_path"),
-           "Molecule from a Gaussian formatted checkpoint (.fchk) or Molden (.molden) file.")
+           "Molecule from a Gaussian formatted checkpoint (.fchk), Molden (.molden) or AIM (.wfn, .wfx) file.")
       .def_static("from_fchk", &Molecule::from_fchk, py::arg("file_path"))
       .def_static("from_arrays", &Molecule::from_arrays, py::arg("centers"), py::arg("shell_atom"),
                   py::arg("nprim"), py::arg("nseg"), py::arg("angmoms"), py::arg("exps"),

@@ -143,9 +143,22 @@ int ctc_molecule_create_from_fchk(const char* path, ctc_molecule** out);
  * (Molden's Cartesian g order is permuted), and the density matrix
  * sum_i occ_i c_i c_i^T over the [MO] orbitals with their occupations. */
 int ctc_molden_load(const char* path, ctc_fchk** out);
+
+/* ---- AIM wavefunction files (.wfn, .wfx) ---------------------------------------
+ * The primitive-based formats the reference's Molecule(str) also accepts
+ * through iodata (src/pymolecule.cu:18-23).  Every distinct (centre, l,
+ * exponent) of the file's primitives becomes a one-primitive Cartesian shell;
+ * orbital coefficients, which multiply unnormalised primitives in these
+ * files, are rescaled to the library's normalised functions, and the density
+ * matrix is sum_i occ_i c_i c_i^T.  The .wfx form is recognised by its tags.
+ * Primitive types 1-20 (s to f); g primitives are refused.  Fills the same
+ * ctc_fchk handle as ctc_fchk_load. */
+int ctc_wfn_load(const char* path, ctc_fchk** out);
+
 /* ctc_molecule_create from a wavefunction file, by extension: .molden,
- * .molden.input and .mold are read as Molden files, anything else as fchk.
- * Replaces Molecule(str) (src/pymolecule.cu:18-23). */
+ * .molden.input and .mold are read as Molden files, .wfn and .wfx as AIM
+ * wavefunction files, anything else as fchk.  Replaces Molecule(str)
+ * (src/pymolecule.cu:18-23). */
 int ctc_molecule_create_from_file(const char* path, ctc_molecule** out);
 
 /* ---- local descriptors --------------------------------------------------------------------- */

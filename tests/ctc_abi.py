@@ -79,17 +79,20 @@ def lib():
         L.ctc_fchk_destroy.restype = None
         L.ctc_molecule_create_from_fchk.argtypes = [C.c_char_p, vp]
         L.ctc_molden_load.argtypes = [C.c_char_p, vp]
+        L.ctc_wfn_load.argtypes = [C.c_char_p, vp]
         L.ctc_molecule_create_from_file.argtypes = [C.c_char_p, vp]
     return _lib
 
 
-def load_fchk(path: str, molden: bool = False) -> dict:
+def load_fchk(path: str, molden: bool = False, wfn: bool = False) -> dict:
     """Basis (flat layout of synthetic.flatten_basis), atoms and density matrix of an .fchk
-    (or, with molden=True, a Molden) file as read by the library's native reader (host only,
+    (or, with molden=True, a Molden; with wfn=True, a .wfn/.wfx) file as read by the library's native reader (host only,
     no GPU needed)."""
     h = C.c_void_p()
     if molden:
         check(lib().ctc_molden_load(path.encode(), C.byref(h)), "ctc_molden_load")
+    elif wfn:
+        check(lib().ctc_wfn_load(path.encode(), C.byref(h)), "ctc_wfn_load")
     else:
         check(lib().ctc_fchk_load(path.encode(), C.byref(h)), "ctc_fchk_load")
     try:
@@ -118,6 +121,11 @@ def load_fchk(path: str, molden: bool = False) -> dict:
 
 def load_molden(path: str) -> dict:
     return load_fchk(path, molden=True)
+
+
+def load_wfn(path: str) -> dict:
+    """A .wfn or .wfx file through ctc_wfn_load (host only)."""
+    return load_fchk(path, wfn=True)
 
 
 def err() -> str:
