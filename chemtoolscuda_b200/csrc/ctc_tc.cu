@@ -298,6 +298,37 @@ __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int
   }
 }
 
+// One nu tile of the contraction for NQA = 1 (rows are the tile's 128
+// points; thread etid owns point etid): acc[q] += sum_nu G[nu][etid] A_q[nu]
+// for the NQ AO quantities, the columns in order.  The AO values stream in
+// groups of GW columns through 4 register buffers (3 groups in flight).
+template <int NQ, int GW>
+__device__ __forceinline__ void contract_rows(const double* __restrict__ ao, int64_t ldq,
+                                              const double* __restrict__ sG, int etid, uint64_t stream,
+                                              double* acc) {
+  constexpr int NB = 4;
+  constexpr int NG = kN / GW;
+  double a[NB][NQ][GW];
+  auto load = [&](int buf, int cg) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int j = 0; j < GW; ++j) a[buf][q][j] = ldg_f64_stream(ao + q * ldq + (cg + j) * kRows, stream);
+  };
+#pragma unroll
+  for (int g = 0; g < NB - 1; ++g) load(g, g * GW);
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    if (g + NB - 1 < NG) load((g + NB - 1) % NB, (g + NB - 1) * GW);
+#pragma unroll
+    for (int j = 0; j < GW; ++j) {
+      const double gv = sG[(g * GW + j) * kRows + etid];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) acc[q] = fma(gv, a[g % NB][q][j], acc[q]);
+    }
+  }
+}
+
 template <int ROLE>
 __device__ __forceinline__ void store_role(double (*s_sums)[16], int lane, const double* acc) {
   constexpr int NS = role_nslot(ROLE);
@@ -671,13 +702,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           }
         } else {
           // rows are points: sums over the nq_ao (1 or 4) quantities of this point
-#pragma unroll 4
-          for (int c = 0; c < kN; ++c) {
-            const double g = sG[c * kRows + etid];
-#pragma unroll
-            for (int qq = 0; qq < 4; ++qq)
-              if (qq < nq_ao) acc[qq] = fma(g, ldg_f64_stream(ao_nt + qq * ldq + c * PTS, stream), acc[qq]);
-          }
+          if (nq_ao == 1) contract_rows<1, 4>(ao_nt, ldq, sG, etid, stream, acc);
+          else contract_rows<4, 2>(ao_nt, ldq, sG, etid, stream, acc);
         }
         if (args.trace) {
           // results of the contraction are complete when they are used
