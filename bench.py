@@ -246,12 +246,14 @@ def fp64_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def profile_traffic(name):
-    """Per-launch DRAM bytes of a kernel from a committed ncu summary, if present."""
+def profile_traffic(name, tiles_per_launch):
+    """Per-launch DRAM bytes of a kernel: the committed ncu figure per tile of the benchmark
+    cube (profiles/traffic.json) times the tiles per launch of this step, if present."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
-        d = json.load(open(p))
-        return d.get(name)
+        per_tile = json.load(open(p)).get(name + "_per_tile")
+        if per_tile is not None and tiles_per_launch:
+            return per_tile * tiles_per_launch
     return None
 
 
@@ -321,7 +323,8 @@ def run_ours(args, ws, rank, local):
                     "frac": achieved / peak, "peak_source": peak_src,
                     "fp64_equiv_tflops": 2.0 * macs / (kern_ms * 1e-3) / 1e12,
                     "kernel_ms_per_step": kern_ms, "ao_kernel_ms_per_step": pst[7],
-                    "traffic": profile_traffic("tc_tile_kernel")}
+                    "traffic": profile_traffic("tc_tile_kernel", pst[0] / max(pst[5], 1.0)),
+                    "tiles_per_launch": pst[0] / max(pst[5], 1.0)}
         else:
             peak = fp64_peak_tflops()
             achieved = 2.0 * macs / (kern_ms * 1e-3) / 1e12
@@ -329,7 +332,8 @@ def run_ours(args, ws, rank, local):
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s (fp64)",
                     "frac": achieved / peak, "peak_source": "measured (cuBLAS DGEMM 8192^3)",
                     "kernel_ms_per_step": kern_ms, "ao_kernel_ms_per_step": pst[7],
-                    "traffic": profile_traffic("fp64_tile_kernel")}
+                    "traffic": profile_traffic("fp64_tile_kernel", pst[0] / max(pst[5], 1.0)),
+                    "tiles_per_launch": pst[0] / max(pst[5], 1.0)}
         result = dict(value=value, ms=ms_max / args.steps, stats=st, roof=roof, clocks=clocks, n=n)
 
     # FP64 form of the same step (the metric compares the two forms)
