@@ -34,7 +34,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from chemtoolscuda_b200 import synthetic as S  # noqa: E402
+
+def _load_synthetic():
+    """The seeded workload generator, loaded by file path: importing it through the
+    package would run the package's __init__ and map the library's extension into
+    the process, and the reference arm must run with the reference's code only."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "ctc_bench_synthetic", os.path.join(ROOT, "chemtoolscuda_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+S = _load_synthetic()
 
 SHAPE = (215, 215, 215)
 SPACING = 0.2
@@ -45,6 +58,16 @@ OUT_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon
             "thomas_fermi", "gge", "general_ked")
 METRIC = "grid pts/s for rho, grad rho, Hessian, lap rho, tau_PD, tau_alpha, RDG (TC split vs FP64 form)"
 ALPHA = 0.5
+WORKLOAD = ("c2: 200-atom molecule (pure d/f, 2655 basis functions), 215^3 cubic grid at 0.2 bohr, "
+            "rho+grad+Hessian+lap+tau_PD+tau_alpha(0.5)+RDG")
+
+
+def workload_config(shape, nbasis):
+    """The config object both arms print, so the two lines describe one workload."""
+    return {"workload": WORKLOAD, "nbasis": int(nbasis), "grid": list(shape),
+            "points_per_gpu": int(np.prod(shape)),
+            "l2": "inputs larger than L2: 1.35 GB of outputs per step; basis tables and D stay "
+                  "L2-resident by design"}
 
 
 class Outputs(C.Structure):
@@ -311,6 +334,9 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     pst = stats(lib, h)
     check(lib, lib.ctc_molecule_set_profiling(h, 0), "profiling")
+    # outputs of that step at the CPU baseline's sample points, for the parity block
+    sample_idx = np.random.default_rng(7).choice(n, min(args.cpu_points, n), replace=False)
+    sample_got = _gather(outs, sample_idx)
     macs = pst[3]                      # sum over tiles of rows * kt^2
     kern_ms = pst[6]
     result = None
@@ -339,16 +365,19 @@ def run_ours(args, ws, rank, local):
     # FP64 form of the same step (the metric compares the two forms)
     fp64 = None
     if prec == 1 and not args.no_fp64_form:
+        fsteps = max(1, min(args.steps, 3))
         step(0)
         torch.cuda.synchronize()
         barrier(ws)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        step(0)
+        for _ in range(fsteps):
+            step(0)
         e1.record()
         torch.cuda.synchronize()
-        fms = allreduce_max(e0.elapsed_time(e1), ws)
-        fp64 = {"value": ws * n / (fms * 1e-3), "ms_per_step": fms, "steps": 1}
+        fms = allreduce_max(e0.elapsed_time(e1), ws) / fsteps
+        fp64 = {"value": ws * n / (fms * 1e-3), "ms_per_step": fms, "steps": fsteps,
+                "_sample": _gather(outs, sample_idx)}
 
     # end to end through the C ABI with host buffers (copies inside the timed region)
     e2e = None
@@ -375,7 +404,7 @@ def run_ours(args, ws, rank, local):
         mol5 = S.make_molecule("c5", seed=0)
         h5 = create(lib, mol5)
         sp = S.surface_points(mol5, seed=0)
-        m = min(len(sp), args.esp_points)
+        m = len(sp) if args.esp_points <= 0 else min(len(sp), args.esp_points)
         p5 = torch.as_tensor(np.ascontiguousarray(sp[:m]), device="cuda")
         o5 = torch.empty(m, dtype=torch.float64, device="cuda")
         check(lib, lib.ctc_eval_esp(h5, p5.data_ptr(), m, o5.data_ptr(), stream), "esp")
@@ -390,22 +419,66 @@ def run_ours(args, ws, rank, local):
                "surface_points_total": int(len(sp)), "nbasis": mol5.nbasis, "atoms": 100}
         lib.ctc_molecule_destroy(h5)
 
-    # CPU baseline: the FP64 oracle on this host's cores, bounded sample of the same grid
+    # CPU baseline: the FP64 oracle on this host's cores, bounded sample of the same grid;
+    # its outputs are also the checker of the parity block (GPU outputs at the same points)
     cpu = None
+    parity = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         from oracle import oracle as O
-        rng = np.random.default_rng(7)
-        allp = S.cube_points(origin, axes, shape)
-        sample = allp[rng.choice(n, args.cpu_points, replace=False)]
+        sample = S.cube_points(origin, axes, shape)[sample_idx]
         t0 = time.perf_counter()
-        O.eval_local(mol.flat(), mol.D, sample, alpha=ALPHA,
-                     keys=("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg"))
+        ref = O.eval_local(mol.flat(), mol.D, sample, alpha=ALPHA, keys=KEYS)
         el = time.perf_counter() - t0
-        cpu = {"value": args.cpu_points / el, "unit": "grid points/s", "cores": os.cpu_count(),
-               "kind": "port", "sample": f"{args.cpu_points} random points of the 215^3 grid, "
-                                          "all seven descriptors, FP64 C++/OpenMP oracle"}
+        cpu = {"value": len(sample) / el, "unit": "grid points/s", "cores": os.cpu_count(),
+               "kind": "port", "sample": f"{len(sample)} random points of the 215^3 grid (seeded), "
+                                          "all seven descriptors, FP64 C++/OpenMP oracle on all "
+                                          "host threads"}
+        parity = _parity_block(mol, sample, ref, sample_got, fp64["_sample"] if fp64 else None)
+    if fp64:
+        fp64.pop("_sample", None)
     lib.ctc_molecule_destroy(h)
-    return result, fp64, e2e, esp, cpu, mol.nbasis
+    return result, fp64, e2e, esp, cpu, parity, mol.nbasis
+
+
+def _gather(outs, idx):
+    """Host copies of the device outputs at flat grid indices idx."""
+    import torch
+    it = torch.as_tensor(np.asarray(idx, np.int64), device="cuda")
+    res = {}
+    for k, t in outs.items():
+        a = t.view(-1, WIDTH[k])[it].cpu().numpy()
+        res[k] = a.reshape(-1, 3) if k == "grad" else (a.reshape(-1, 3, 3) if k == "hess" else a.ravel())
+    return res
+
+
+def _parity_block(mol, pts, ref, got_tc, got_fp64, chunk=500):
+    """Largest error of every timed output over the CPU baseline's sample, relative
+    to the per-point sum of absolute terms (the measure the tests use), for the
+    tensor-core step and the FP64 form; RDG where rho > 1e-10."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import term_scales
+    parts = [term_scales(mol.flat(), mol.D, pts[i:i + chunk], alpha=ALPHA,
+                         ref={k: v[i:i + chunk] for k, v in ref.items()})
+             for i in range(0, len(pts), chunk)]
+    sc = {k: np.concatenate([p[k] for p in parts]) for k in KEYS}
+    live = ref["rho"] > 1e-10
+
+    def errs(got):
+        out = {}
+        for k in KEYS:
+            e = np.maximum(np.abs(got[k] - ref[k]) - PARITY_ATOL, 0.0) / np.maximum(sc[k], 1e-300)
+            if k == "rdg":
+                e = e[live]
+            out[k] = float(e.max()) if e.size else 0.0
+        return out
+    blk = {"sample_points": int(len(pts)), "checker": "FP64 oracle (the cpu_baseline run)",
+           "measure": "max |x - x_oracle| / sum of |terms| per output (atol 1e-14; RDG where rho > 1e-10)",
+           "tolerance": {"tc": 1e-8, "fp64": 1e-10}, "tc": errs(got_tc)}
+    if got_fp64 is not None:
+        blk["fp64"] = errs(got_fp64)
+    blk["pass"] = all(v <= 1e-8 for v in blk["tc"].values()) and (
+        got_fp64 is None or all(v <= 1e-10 for v in blk["fp64"].values()))
+    return blk
 
 
 # --------------------------------------------------------------------------- reference arm
@@ -434,11 +507,13 @@ def run_reference(args, ws, rank):
     shape = tuple(args.shape)
     origin, axes = S.cube_grid(mol, SPACING, shape)
     allp = S.cube_points(origin, axes, shape)
-    n = args.ref_points
-    rng = np.random.default_rng(11)
     M = mol.nbasis
-    # the reference indexes with 32-bit integers: keep 6 * M * n below 2^31
-    assert 6 * M * n < 2 ** 31
+    # the reference indexes its AO arrays with 32-bit integers (src/evaluate_hessian.cu:21,30):
+    # the Hessian's 6 M x n second-derivative array must stay below 2^31 entries, so the
+    # largest legal batch is used unless --ref-points asks for fewer
+    n_max = (2 ** 31 - 1) // (6 * M)
+    n = min(args.ref_points, n_max) if args.ref_points > 0 else n_max
+    rng = np.random.default_rng(11)
 
     def step(pts):
         outs = {"density": np.empty(n), "gradient": np.empty((n, 3)), "hessian": np.empty((n, 3, 3)),
@@ -464,11 +539,17 @@ def run_reference(args, ws, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": "c2: 200-atom molecule, 215^3 grid at 0.2 bohr, all local descriptors",
-                       "nbasis": M, "points_per_step": n,
-                       "reference_calls": "evaluate_electron_density_on_any_grid, _gradient, _hessian, "
-                                          "evaluate_laplacian, evaluate_positive_definite_kinetic_density, "
-                                          "evaluate_general_kinetic_energy_density, compute_reduced_density_gradient"},
+            "config": workload_config(shape, M),
+            "reference_sampling": {
+                "points_per_step": n, "largest_legal_batch": n_max,
+                "why": "a full 215^3 step would take minutes on the reference; each step is a seeded "
+                       "random sample of the same grid, at the largest batch its 32-bit AO indexing "
+                       "allows, and the metric (points/s) is per point",
+                "calls_per_step": "evaluate_electron_density_on_any_grid, evaluate_electron_density_gradient, "
+                                  "evaluate_electron_density_hessian, evaluate_laplacian, "
+                                  "evaluate_positive_definite_kinetic_density, "
+                                  "evaluate_general_kinetic_energy_density, compute_reduced_density_gradient",
+                "timing": "wall clock around the reference's synchronous host API (host arrays in and out)"},
             "cpu_baseline": {"value": value, "unit": "grid points/s", "cores": 1, "kind": "reference",
                              "sample": f"{n} random points of the 215^3 grid per step; the reference is "
                                        "CUDA code (no CPU implementation): its own drivers built from "
@@ -702,9 +783,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-esp", action="store_true")
     ap.add_argument("--no-fp64-form", action="store_true")
-    ap.add_argument("--cpu-points", type=int, default=1500)
-    ap.add_argument("--esp-points", type=int, default=20000)
-    ap.add_argument("--ref-points", type=int, default=16384)
+    ap.add_argument("--cpu-points", type=int, default=10000)
+    ap.add_argument("--esp-points", type=int, default=0,
+                    help="ESP leg points (0: the whole surface set of the 100-atom molecule)")
+    ap.add_argument("--ref-points", type=int, default=0,
+                    help="reference arm points per step (0: the largest batch its 32-bit indexing allows)")
     ap.add_argument("--workload", default=None, choices=["c1", "c3", "c4", "c5"],
                     help="measure another configuration instead of the headline one (one GPU)")
     args = ap.parse_args()
@@ -724,7 +807,7 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return 0
-    res, fp64, e2e, esp, cpu, nbasis = run_ours(args, ws, rank, local)
+    res, fp64, e2e, esp, cpu, parity, nbasis = run_ours(args, ws, rank, local)
     if rank == 0:
         dtype = ("int8 digit split (5 AO x 4 D digits), exact int32 accumulation, fp64 AO/epilogue"
                  if args.precision == "tc" else "f64")
@@ -733,16 +816,15 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
             "data": "synthetic",
-            "config": {"workload": "c2: 200-atom molecule (pure d/f), 215^3 cubic grid at 0.2 bohr, "
-                                   "rho+grad+Hessian+lap+tau_PD+tau_alpha(0.5)+RDG",
-                       "nbasis": nbasis, "points_per_gpu": res["n"], "precision": args.precision,
-                       "l2": "outputs of one step (1.35 GB) exceed L2; basis tables and D stay L2-resident by design",
-                       "tiles_per_step": res["stats"][0] / args.steps,
-                       "mean_compact_aos_per_tile": res["stats"][2] / max(res["stats"][0], 1)},
-            "roofline": res["roof"], "cpu_baseline": cpu, "e2e": e2e,
+            "config": workload_config(args.shape, nbasis),
+            "pipeline": {"precision": args.precision, "tiles_per_step": res["stats"][0] / args.steps,
+                         "mean_compact_aos_per_tile": res["stats"][2] / max(res["stats"][0], 1)},
+            "roofline": res["roof"], "cpu_baseline": cpu, "parity": parity, "e2e": e2e,
             "gpu_launches": int(res["stats"][4]), "clocks": res["clocks"],
             "fp64_form": fp64, "esp": esp,
         }
+        if fp64:
+            line["tc_over_fp64"] = res["value"] / fp64["value"]
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

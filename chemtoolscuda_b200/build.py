@@ -36,6 +36,7 @@ CU_SOURCES = ["ctc_basis.cu", "ctc_ao.cu", "ctc_local.cu", "ctc_tc.cu", "ctc_esp
               "ctc_adjoint.cu", "ctc_api.cu", "ctc_noalloc.cu", "ctc_fchk.cpp",
               "ctc_molden.cpp", "ctc_wfn.cpp"]
 HEADERS = ["ctc_internal.h", "ctc_terms.inc", "ctc_ao_poly.inc", "ctc_tiles.cuh", "ctc_split.cuh",
+           "ctc_finalize.cuh",
            "ctc_wfnfile.h"]
 
 

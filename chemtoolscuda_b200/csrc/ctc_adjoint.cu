@@ -154,14 +154,12 @@ int eval_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const dou
     Cacc = (double*)mol->ws_sl.p;
     CTC_CUDA_TRY(cudaMemsetAsync(Cacc, 0, cbytes, st));
   }
-  static bool attr[2] = {false, false};
-  if (dLdR && !attr[nqa == 4]) {
-    if (nqa == 4)
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
-    else
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
-    attr[nqa == 4] = true;
+  if (dLdR) {
+    rc = nqa == 4 ? ensure_smem_attr((const void*)fp64_tile_kernel<4, 1>, (int)kSmemFp64)
+                  : ensure_smem_attr((const void*)fp64_tile_kernel<1, 1>, (int)kSmemFp64);
+    if (rc != CTC_OK) return rc;
   }
+  if (dLdD && (rc = ensure_smem_attr((const void*)gemm_tn_kernel, kSmemTn)) != CTC_OK) return rc;
   ForceArgs fa;
   fa.v_rho = v_rho;
   fa.v_grad = v_grad;
@@ -200,11 +198,6 @@ int eval_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const dou
       kchunk = (kchunk + TN_BK - 1) / TN_BK * TN_BK;
       splits = (int)((rows + kchunk - 1) / kchunk);
       dim3 grid(Mpad / TN_BN, Mpad / TN_BM, splits);
-      static bool tn_attr = false;
-      if (!tn_attr) {
-        CTC_CUDA_TRY(cudaFuncSetAttribute(gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTn));
-        tn_attr = true;
-      }
       gemm_tn_kernel<<<grid, 256, kSmemTn, st>>>(Phi, W, rows, Mpad, kchunk, Cacc);
       CTC_CUDA_TRY(cudaGetLastError());
       mol->host_launches += 2;

@@ -198,6 +198,9 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
   }
   drain(b);
   drain(b ^ 1);
+  // a device-side failure of the tensor-core kernels of this call
+  if (rc == CTC_OK && cs && precision == CTC_PREC_TC_SPLIT)
+    rc = check_status(mol, cs, "ctc_eval_local_host");
   if (cs) cudaStreamSynchronize(cs);
   if (h2d) cudaStreamSynchronize(h2d);
   if (d2h) cudaStreamSynchronize(d2h);

@@ -10,9 +10,11 @@
 // the adjoint.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 #include "ctc_internal.h"
 
@@ -27,6 +29,43 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
   return code;
+}
+
+// Kernel attributes are per device: a kernel launched on a second GPU needs its
+// own cudaFuncSetAttribute.  One entry per (device, kernel, bytes) that has
+// been configured, under a mutex so that host threads may call in together.
+namespace {
+std::mutex g_attr_mu;
+std::vector<std::tuple<int, const void*, int>> g_attr_done;
+std::mutex g_sm_mu;
+std::vector<std::pair<int, int>> g_sm_count;  // (device, SM count)
+}  // namespace
+
+int ensure_smem_attr(const void* kernel, int bytes) {
+  int dev = 0;
+  CTC_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  const auto key = std::make_tuple(dev, kernel, bytes);
+  if (std::find(g_attr_done.begin(), g_attr_done.end(), key) != g_attr_done.end()) return CTC_OK;
+  CTC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  g_attr_done.push_back(key);
+  return CTC_OK;
+}
+
+int device_sm_count(int* out) {
+  int dev = 0;
+  CTC_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_sm_mu);
+  for (const auto& e : g_sm_count)
+    if (e.first == dev) {
+      *out = e.second;
+      return CTC_OK;
+    }
+  int n = 0;
+  CTC_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  g_sm_count.push_back({dev, n});
+  *out = n;
+  return CTC_OK;
 }
 
 int type_of_angmom(int am) {
@@ -53,8 +92,23 @@ int l_of_type(int t) {
   return (t >= 0 && t < kNumTypes) ? l[t] : -1;
 }
 
+// CTC_SCRATCH_LIMIT_BYTES caps every scratch allocation of a molecule: a
+// larger request fails with CTC_ERR_NOMEM as if the device were out of
+// memory (a bound for a process sharing the GPU, and the way the tests make
+// the out-of-memory path run).
+static size_t scratch_limit() {
+  const char* e = std::getenv("CTC_SCRATCH_LIMIT_BYTES");
+  if (!e) return 0;
+  const long long v = std::atoll(e);
+  return v > 0 ? (size_t)v : 0;
+}
+
 int Scratch::ensure(size_t need, cudaStream_t st) {
   if (need <= bytes) return CTC_OK;
+  const size_t lim = scratch_limit();
+  if (lim && need > lim)
+    return fail(CTC_ERR_NOMEM, "scratch allocation of " + std::to_string(need) +
+                                   " bytes exceeds CTC_SCRATCH_LIMIT_BYTES = " + std::to_string(lim));
   if (p) {
     cudaError_t e = cudaFreeAsync(p, st);
     if (e != cudaSuccess) return fail(CTC_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(e));
@@ -88,15 +142,53 @@ int64_t chunk_points(const ctc_molecule* mol, int nq_ao) {
   return (n / 128) * 128;
 }
 
-int check_status(ctc_molecule* mol, cudaStream_t st, const char* what) {
-  int32_t h = 0;
-  CTC_CUDA_TRY(cudaMemcpyAsync(&h, mol->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  CTC_CUDA_TRY(cudaStreamSynchronize(st));
-  if (h != 0) {
-    cudaMemsetAsync(mol->d_status, 0, sizeof(int32_t), st);
-    return fail(CTC_ERR_DEVICE, std::string(what) + ": kernel status " + std::to_string(h));
-  }
+// The status word.  Kernels that can fail on the device (bounded waits of the
+// tensor-core pipeline) set the molecule's device word with atomicExch; it
+// stays set until it is reported.  After such kernels post_status enqueues a
+// copy of it into pinned host memory and records an event, so the call
+// itself never waits.  poll_status (at the start of the next call) reports a
+// copy that has landed; check_status waits for the stream first.
+static std::string status_message(int32_t code) {
+  if (code == 0x7101)
+    return "a bounded wait of the tensor-core contraction ran out (status 0x7101); "
+           "the call's outputs are incomplete";
+  return "kernel status " + std::to_string(code);
+}
+
+static int report_status(ctc_molecule* mol, cudaStream_t st, const char* what) {
+  const int32_t h = *mol->h_status;
+  if (h == 0) return CTC_OK;
+  *mol->h_status = 0;
+  mol->status_pending = false;
+  CTC_CUDA_TRY(cudaMemsetAsync(mol->d_status, 0, sizeof(int32_t), st));
+  return fail(CTC_ERR_DEVICE, std::string(what) + ": " + status_message(h));
+}
+
+int post_status(ctc_molecule* mol, cudaStream_t st) {
+  CTC_CUDA_TRY(cudaMemcpyAsync(mol->h_status, mol->d_status, sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, st));
+  CTC_CUDA_TRY(cudaEventRecord(mol->status_ev, st));
+  mol->status_pending = true;
   return CTC_OK;
+}
+
+int poll_status(ctc_molecule* mol, cudaStream_t st) {
+  if (!mol->status_pending) return CTC_OK;
+  const cudaError_t q = cudaEventQuery(mol->status_ev);
+  if (q == cudaErrorNotReady) return CTC_OK;
+  CTC_CUDA_TRY(q);
+  mol->status_pending = *mol->h_status != 0;
+  return report_status(mol, st, "an earlier call on this molecule");
+}
+
+int check_status(ctc_molecule* mol, cudaStream_t st, const char* what) {
+  CTC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (mol->status_pending) CTC_CUDA_TRY(cudaEventSynchronize(mol->status_ev));
+  int32_t h = 0;
+  CTC_CUDA_TRY(cudaMemcpy(&h, mol->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (h != 0 && *mol->h_status == 0) *mol->h_status = h;
+  mol->status_pending = false;
+  return report_status(mol, st, what);
 }
 
 // Radius beyond which |AO|, |grad AO| and |hess AO| of a segment stay below
@@ -318,6 +410,8 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
 #undef ALLOC_COPY
   if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
       cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess ||
+      cudaMallocHost((void**)&m->h_status, sizeof(int32_t)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&m->status_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc((void**)&m->d_stats, sizeof(double) * 8) != cudaSuccess ||
       cudaMemset(m->d_stats, 0, sizeof(double) * 8) != cudaSuccess) {
     ctc_molecule_destroy(m);
@@ -342,6 +436,8 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   cudaFree(m->d_Dsl);
   cudaFree(m->d_Dscale);
   cudaFree(m->d_status);
+  if (m->h_status) cudaFreeHost(m->h_status);
+  if (m->status_ev) cudaEventDestroy(m->status_ev);
   cudaFree(m->d_stats);
   m->ws_ao.release();
   m->ws_sl.release();
@@ -418,6 +514,18 @@ int ctc_molecule_get_stats(ctc_molecule* m, double* stats) {
 int ctc_molecule_set_profiling(ctc_molecule* m, int32_t on) {
   if (!m) return fail(CTC_ERR_INVALID, "set_profiling: null molecule");
   m->prof = on != 0;
+  return CTC_OK;
+}
+
+int ctc_molecule_sync_status(ctc_molecule* m, void* stream) {
+  if (!m) return fail(CTC_ERR_INVALID, "sync_status: null molecule");
+  return check_status(m, (cudaStream_t)stream, "device status");
+}
+
+int ctc_molecule_set_wait_limit(ctc_molecule* m, int64_t cycles) {
+  if (!m) return fail(CTC_ERR_INVALID, "set_wait_limit: null molecule");
+  if (cycles < 0) return fail(CTC_ERR_INVALID, "set_wait_limit: negative cycle count");
+  m->wait_cycles = cycles;
   return CTC_OK;
 }
 

@@ -14,6 +14,13 @@ namespace ctc {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 
+// Sets a kernel's dynamic shared-memory limit once per (device, kernel, size):
+// the attribute is per device, so every device a kernel runs on needs it.
+// Thread-safe.  kernel is the __global__ function's address.
+int ensure_smem_attr(const void* kernel, int bytes);
+// Streaming multiprocessors of the current device (cached per device).
+int device_sm_count(int* out);
+
 #define CTC_CUDA_TRY(expr)                                                               \
   do {                                                                                   \
     cudaError_t _e = (expr);                                                             \
@@ -133,8 +140,14 @@ struct ctc_molecule {
   int8_t* d_Dsl = nullptr;
   double* d_Dscale = nullptr;
   bool dsl_valid = false;
-  // per-call status word written by kernels
+  // status word written by kernels (sticky until reported), its pinned host
+  // copy, and the event recorded after the copy was enqueued
   int32_t* d_status = nullptr;
+  int32_t* h_status = nullptr;
+  cudaEvent_t status_ev = nullptr;
+  bool status_pending = false;
+  // limit of the tensor-core pipeline's waits in SM cycles (0: the default)
+  int64_t wait_cycles = 0;
   // work counters: [0] tiles [1] points [2] sum kt_true [3] sum rows*kt^2 (device, doubles)
   double* d_stats = nullptr;
   double host_launches = 0, host_chunks = 0;
@@ -203,7 +216,11 @@ int eval_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const dou
 // chunk size (points) for a given AO footprint
 int64_t chunk_points(const ctc_molecule* mol, int nq_ao);
 
-// status word helpers
+// status word helpers: post_status enqueues the copy of the word after the
+// kernels just launched (no wait), poll_status reports a landed copy without
+// waiting, check_status synchronises the stream and reports
+int post_status(ctc_molecule* mol, cudaStream_t st);
+int poll_status(ctc_molecule* mol, cudaStream_t st);
 int check_status(ctc_molecule* mol, cudaStream_t st, const char* what);
 
 // Records a start/stop event pair around a launch when profiling is on.

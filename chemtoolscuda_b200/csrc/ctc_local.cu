@@ -42,20 +42,12 @@ LocalPlan plan_local(const ctc_outputs* o) {
 int fp64_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                      const ctc_params* prm, const ctc_outputs* out, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
-  static bool attr_set[2] = {false, false};
+  int rc;
   if (plan.nqa == 4) {
-    if (!attr_set[1]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<4, 0>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
-      attr_set[1] = true;
-    }
+    if ((rc = ensure_smem_attr((const void*)fp64_tile_kernel<4, 0>, (int)kSmemFp64)) != CTC_OK) return rc;
     fp64_tile_kernel<4, 0><<<tb.C, kThreads, kSmemFp64, st>>>(tb, mol->d_D, mol->Mpad, *out, *prm, ForceArgs{});
   } else {
-    if (!attr_set[0]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(fp64_tile_kernel<1, 0>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemFp64));
-      attr_set[0] = true;
-    }
+    if ((rc = ensure_smem_attr((const void*)fp64_tile_kernel<1, 0>, (int)kSmemFp64)) != CTC_OK) return rc;
     fp64_tile_kernel<1, 0><<<tb.C, kThreads, kSmemFp64, st>>>(tb, mol->d_D, mol->Mpad, *out, *prm, ForceArgs{});
   }
   CTC_CUDA_TRY(cudaGetLastError());
@@ -72,8 +64,10 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
     return fail(CTC_ERR_INVALID, "eval_local: at most 2^31-1 points per call");
   const LocalPlan plan = plan_local(out);
   if (precision == CTC_PREC_TC_SPLIT) {
-    int rc = prepare_tc(mol, st);
+    // a failure an earlier stream-ordered call recorded on the device
+    int rc = poll_status(mol, st);
     if (rc != CTC_OK) return rc;
+    if ((rc = prepare_tc(mol, st)) != CTC_OK) return rc;
   }
   const int TP = 128 / plan.nqa;
   // tensor-core path: the AO kernel also writes the int8 digit planes
@@ -100,8 +94,9 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
       },
       precision == CTC_PREC_TC_SPLIT ? &sliced_ao : nullptr);
   if (rc != CTC_OK) return rc;
-  // the tensor-core kernels report bounded-wait timeouts through the status word
-  if (precision == CTC_PREC_TC_SPLIT) return check_status(mol, st, "tensor-core contraction");
+  // the tensor-core kernels report bounded-wait timeouts through the status
+  // word: its copy is enqueued here and read by a later call (no wait now)
+  if (precision == CTC_PREC_TC_SPLIT) return post_status(mol, st);
   return CTC_OK;
 }
 

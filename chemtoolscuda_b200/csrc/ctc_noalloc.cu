@@ -113,7 +113,8 @@ int eval_local_noalloc(ctc_molecule* mol, const double* d_points, int64_t n, con
   size_t sort_tmp = 0;
   CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (uint32_t*)nullptr,
                                                (uint32_t*)nullptr, (int32_t*)nullptr,
-                                               (int32_t*)nullptr, (int)n, 0, 30, st));
+                                               (int32_t*)nullptr, (int)n, 0, kMortonSortBits,
+                                               st));
   Carve cv{(char*)base};
   uint32_t* k_in = cv.take<uint32_t>(n);
   uint32_t* k_out = cv.take<uint32_t>(n);
@@ -165,7 +166,7 @@ int eval_local_noalloc(ctc_molecule* mol, const double* d_points, int64_t n, con
                                                               1024.0 / ext, k_in, v_in);
   CTC_CUDA_TRY(cudaGetLastError());
   CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, sort_tmp, k_in, k_out, v_in, perm, (int)n, 0,
-                                               30, st));
+                                               kMortonSortBits, st));
   mol->host_launches += 2;
   for (int64_t t0 = 0; t0 < ntiles; t0 += C) {
     tb.C = (int)std::min<int64_t>(C, ntiles - t0);

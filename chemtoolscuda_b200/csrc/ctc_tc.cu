@@ -46,6 +46,7 @@
 
 #include "ctc_internal.h"
 #include "ctc_split.cuh"
+#include "ctc_finalize.cuh"
 
 namespace ctc {
 
@@ -91,11 +92,13 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
-// Bounded wait on an mbarrier phase: false after ~2 s of GPU time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait on an mbarrier phase: false once `limit` SM cycles have passed
+// (the pipeline's waits take the launch's limit, by default kWaitCycles).
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9-2.0 GHz
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kWaitCycles) {
   const uint32_t a = smem_u32(bar);
   const long long t0 = clock64();
-  for (uint32_t it = 0;; ++it) {
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -104,7 +107,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 255) == 255 && clock64() - t0 > 4000000000LL) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
@@ -379,21 +382,23 @@ struct TcArgs {
   // first); tile_counter (zero at launch) hands them out to the CTAs
   const int32_t* order;
   int32_t* tile_counter;
+  // limit of every pipeline wait, in SM cycles (kWaitCycles unless a caller
+  // shortens it to exercise the timeout path)
+  long long wait_cycles;
   // optional per-CTA cycle counters (CTC_TC_TRACE): [grid][8] = total,
   // producer wait on empty, producer stage work, MMA wait on full, MMA wait
   // on tempty, epilogue wait on tfull, drain, contraction
   long long* trace;
 };
 
-__device__ __forceinline__ void finalize_point_tc(const double* s, int nqa, int nq_ao,
-                                                  const ctc_outputs& o, int64_t idx,
-                                                  const ctc_params& prm);
-
 template <int NQA>
 __global__ void __launch_bounds__(kThreadsTc, 1)
     tc_tile_kernel(const __grid_constant__ CUtensorMap amap, TcArgs args) {
   extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
+  // full_bar[s]: the 128 producer threads wrote stage s's B planes; tma_bar[s]:
+  // stage s's A planes landed (its own barrier, so that an exit after a
+  // timeout can wait for exactly the TMA loads it issued)
+  __shared__ __align__(8) uint64_t full_bar[kStages], tma_bar[kStages], empty_bar[kStages];
   __shared__ __align__(8) uint64_t tfull_bar, tempty_bar, done_bar;
   __shared__ __align__(8) uint64_t tile_full_bar[2], tile_empty_bar[2];
   __shared__ uint32_t tmem_base_sh;
@@ -414,7 +419,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], 129);
+      mbar_init(&full_bar[s], 128);
+      mbar_init(&tma_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
     mbar_init(&tfull_bar, 1);
@@ -443,16 +449,28 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   // the launch-wide counter, publishes it (-1 when the chunk is exhausted) and
   // every role reads it; a slot is refilled once all kTileReaders readers have
   // released it.  Each role walks the same tile sequence at its own pace.
+  //
+  // Abort decisions are warp-uniform: a warp takes every decision that leads
+  // to a warp-collective instruction (__syncwarp, shuffles, tcgen05 .aligned
+  // forms) from one vote, so lanes whose waits end at different moments (a
+  // timeout in one lane only) never split around such an instruction.
   auto read_tile = [&](int i) -> int {
     const int slot = i & 1;
     int t = -1;
-    if (!mbar_wait(&tile_full_bar[slot], (i >> 1) & 1)) {
+    if (!mbar_wait(&tile_full_bar[slot], (i >> 1) & 1, args.wait_cycles)) {
       s_abort = 1;
     } else {
       t = s_tile[slot];
     }
     return t;
   };
+  // whole-warp form: lane 0 waits, the warp takes its answer
+  auto read_tile_warp = [&](int i) -> int {
+    int t = -1;
+    if (lane == 0) t = read_tile(i);
+    return __shfl_sync(0xffffffffu, t, 0);
+  };
+  auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, s_abort != 0); };
 
   if (warp < 4) {
     // ---------------- producers
@@ -466,11 +484,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     const int k4 = (tid & 15) * 4, nrow0 = tid >> 4;
     const uint64_t keep = policy_evict_last();
     int it = 0;  // stage counter across tiles
+    // thread 0: stage counter of the last TMA issue into each slot (-1: none)
+    int last_issue[kStages];
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) last_issue[s] = -1;
     for (int i = 0;; ++i) {
       if (tid == 0) {
         const int slot = i & 1;
         int next = -1;
-        if (!mbar_wait(&tile_empty_bar[slot], ((i >> 1) & 1) ^ 1)) {
+        if (!mbar_wait(&tile_empty_bar[slot], ((i >> 1) & 1) ^ 1, args.wait_cycles)) {
           s_abort = 1;
         } else {
           const int c = atomicAdd(args.tile_counter, 1);
@@ -479,10 +501,9 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         s_tile[slot] = next;
         mbar_arrive(&tile_full_bar[slot]);
       }
-      const int t = read_tile(i);
-      __syncwarp();
+      const int t = read_tile_warp(i);
       if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
-      if (t < 0 || s_abort) break;
+      if (t < 0 || warp_abort()) break;
       const int kt = tb.kt[t];
       const int nkb = kt / kBK;
       const int nnt = (kt + kN - 1) / kN;
@@ -520,13 +541,17 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         const uint32_t ph = (it / kStages) & 1;
         const int k0 = (j % nkb) * kBK;
         const long long tw = clock64();
-        if (!mbar_wait(&empty_bar[s], ph ^ 1)) { s_abort = 1; break; }
+        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ph ^ 1, args.wait_cycles))) {
+          s_abort = 1;
+          break;
+        }
         tr0 += clock64() - tw;
         if (tid == 0) {
-          mbar_arrive_expect_tx(&full_bar[s], kAStageBytes);
+          mbar_arrive_expect_tx(&tma_bar[s], kAStageBytes);
           for (int p = 0; p < kPlanesA; ++p)
             tma_load_2d_hint(sA + s * kAStageBytes + p * kAPlaneBytes, &amap, k0,
-                             (t * kPlanesA + p) * kRows, &full_bar[s], keep);
+                             (t * kPlanesA + p) * kRows, &tma_bar[s], keep);
+          last_issue[s] = it;
         }
         uint8_t* b = sB + s * kBStageBytes;
 #pragma unroll
@@ -542,7 +567,17 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         mbar_arrive(&full_bar[s]);
         if (more) gather(nu, mu, w);
       }
-      if (s_abort) break;
+      if (warp_abort()) break;
+    }
+    // Before the CTA may exit, every TMA load this thread issued has landed:
+    // on the normal path the MMA warp has already seen each of them complete;
+    // after a timeout a load can still be writing into shared memory.  The
+    // wait uses the full limit, not the launch's (possibly shortened) one.
+    if (tid == 0) {
+#pragma unroll
+      for (int s = 0; s < kStages; ++s)
+        if (last_issue[s] >= 0 && !mbar_wait(&tma_bar[s], (last_issue[s] / kStages) & 1))
+          atomicExch(args.status, (int32_t)kStatusTimeout);
     }
     if (args.trace && tid == 0) {
       args.trace[(int64_t)blockIdx.x * 8 + 1] = tr0;
@@ -561,23 +596,33 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRows >> 4) << 24);
     int it = 0, gnt = 0;  // stage and nu-tile counters across tiles
     for (int i = 0;; ++i) {
-      const int t = read_tile(i);
-      __syncwarp();
+      const int t = read_tile_warp(i);
       if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
-      if (t < 0 || s_abort) break;
+      if (t < 0 || warp_abort()) break;
       const int kt = tb.kt[t];
       const int nkb = kt / kBK;
       const int nnt = (kt + kN - 1) / kN;
-      for (int nt = 0; nt < nnt && !s_abort; ++nt, ++gnt) {
+      bool failed = false;
+      for (int nt = 0; nt < nnt && !failed; ++nt, ++gnt) {
         const long long tw = clock64();
-        if (!mbar_wait(&tempty_bar, (gnt & 1) ^ 1)) { s_abort = 1; break; }
+        if (!__all_sync(0xffffffffu, mbar_wait(&tempty_bar, (gnt & 1) ^ 1, args.wait_cycles))) {
+          s_abort = 1;
+          failed = true;
+          break;
+        }
         tr1 += clock64() - tw;
         tc_fence_after();
         for (int kb = 0; kb < nkb; ++kb, ++it) {
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           const long long tf = clock64();
-          if (!mbar_wait(&full_bar[s], ph)) { s_abort = 1; break; }
+          const bool ready = mbar_wait(&full_bar[s], ph, args.wait_cycles) &&
+                             mbar_wait(&tma_bar[s], ph, args.wait_cycles);
+          if (!__all_sync(0xffffffffu, ready)) {
+            s_abort = 1;
+            failed = true;
+            break;
+          }
           tr0 += clock64() - tf;
           tc_fence_after();
           if (lane == 0) {
@@ -600,11 +645,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
           }
           __syncwarp();
         }
-        if (s_abort) break;
+        if (failed) break;
         if (lane == 0) umma_commit(&tfull_bar);
         __syncwarp();
       }
-      if (s_abort) break;
+      if (failed || warp_abort()) break;
     }
     if (args.trace && lane == 0) {
       args.trace[(int64_t)blockIdx.x * 8 + 3] = tr0;
@@ -661,7 +706,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         // of the previous nu tile
         if (gnt > 0 && s_epi_abort[(gnt - 1) & 1]) { stop = true; break; }
         const long long te = clock64();
-        if (!mbar_wait(&tfull_bar, gnt & 1)) s_abort = 1;
+        if (!mbar_wait(&tfull_bar, gnt & 1, args.wait_cycles)) s_abort = 1;
+        __syncwarp();  // converged for the .aligned TMEM loads below
         const long long td = clock64();
         tr0 += td - te;
         tc_fence_after();
@@ -724,14 +770,22 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         }
         asm volatile("bar.sync 1, 128;\n" ::: "memory");
         if (role == 0 && !aborted) {
-          const int64_t oidx = tb.out[(int64_t)t * tb.TP + lane];
-          if (oidx >= 0) finalize_point_tc(s_sums[lane], 4, nq_ao, args.out, oidx, args.prm);
+          const int64_t pi = (int64_t)t * tb.TP + lane;
+          const int64_t oidx = tb.out[pi];
+          if (oidx >= 0) {
+            if (finite_point(tb.xyz + 3 * pi)) finalize_point(s_sums[lane], 4, nq_ao, args.out, oidx, args.prm);
+            else nan_point(args.out, oidx);
+          }
         }
       } else if (!aborted) {
-        const int64_t oidx = tb.out[(int64_t)t * tb.TP + etid];
+        const int64_t pi = (int64_t)t * tb.TP + etid;
+        const int64_t oidx = tb.out[pi];
         double s16[16];
         for (int q = 0; q < 16; ++q) s16[q] = q < 4 ? acc[q] : 0.0;
-        if (oidx >= 0) finalize_point_tc(s16, 1, nq_ao, args.out, oidx, args.prm);
+        if (oidx >= 0) {
+          if (finite_point(tb.xyz + 3 * pi)) finalize_point(s16, 1, nq_ao, args.out, oidx, args.prm);
+          else nan_point(args.out, oidx);
+        }
       }
     }
     if (args.trace && etid == 0) {
@@ -748,54 +802,10 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     if (lane == 0) umma_commit(&done_bar);
     __syncwarp();
     if (!mbar_wait(&done_bar, 0) && lane == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
+    __syncwarp();  // converged for the .aligned dealloc
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
   }
-}
-
-constexpr double kPi = 3.14159265358979323846;
-
-__device__ __forceinline__ void finalize_point_tc(const double* s, int nqa, int nq_ao,
-                                                  const ctc_outputs& o, int64_t idx,
-                                                  const ctc_params& prm) {
-  const double rho = s[0];
-  const double g0 = 2.0 * s[1], g1 = 2.0 * s[2], g2 = 2.0 * s[3];
-  double H[6] = {0, 0, 0, 0, 0, 0};
-  double tau = 0.0;
-  if (nqa == 4) {
-    for (int i = 0; i < 6; ++i) H[i] = 2.0 * (s[10 + i] + (nq_ao == 10 ? s[4 + i] : 0.0));
-    tau = 0.5 * (s[10] + s[13] + s[15]);
-  }
-  const double lap = H[0] + H[3] + H[5];
-  if (o.rho) o.rho[idx] = rho;
-  if (o.grad) {
-    o.grad[3 * idx] = g0;
-    o.grad[3 * idx + 1] = g1;
-    o.grad[3 * idx + 2] = g2;
-  }
-  if (o.hess) {
-    double* h = o.hess + 9 * idx;
-    h[0] = H[0]; h[1] = H[1]; h[2] = H[2];
-    h[3] = H[1]; h[4] = H[3]; h[5] = H[4];
-    h[6] = H[2]; h[7] = H[4]; h[8] = H[5];
-  }
-  if (o.lap) o.lap[idx] = lap;
-  if (o.tau_pd) o.tau_pd[idx] = tau;
-  if (o.tau_alpha) o.tau_alpha[idx] = tau + prm.alpha * lap;
-  const double gsq = g0 * g0 + g1 * g1 + g2 * g2;
-  if (o.rdg) {
-    const double pref = 0.5 / cbrt(3.0 * kPi * kPi);
-    const double d43 = pow(rho, 4.0 / 3.0);
-    o.rdg[idx] = pref * (d43 > 1e-20 ? sqrt(gsq) / d43 : 1e-20);
-  }
-  if (o.shannon) o.shannon[idx] = rho * log(rho);
-  double w = 0.0, tf = 0.0;
-  if (o.weizsacker || o.gge) w = 8.0 * rho > 1e-20 ? gsq / (8.0 * rho) : 1e-20;
-  if (o.thomas_fermi || o.gge) tf = 0.3 * pow(3.0 * kPi * kPi, 2.0 / 3.0) * pow(rho, 5.0 / 3.0);
-  if (o.weizsacker) o.weizsacker[idx] = w;
-  if (o.thomas_fermi) o.thomas_fermi[idx] = tf;
-  if (o.gge) o.gge[idx] = tf + prm.gge_a * w + prm.gge_b * lap;
-  if (o.general_ked) o.general_ked[idx] = tau + 0.25 * (prm.ked_a - 1.0) * lap;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
@@ -933,12 +943,8 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return fail(CTC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)cr));
-  static int num_sms = 0;
-  if (num_sms == 0) {
-    int dev = 0;
-    CTC_CUDA_TRY(cudaGetDevice(&dev));
-    CTC_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-  }
+  int num_sms = 0;
+  if ((rc = device_sm_count(&num_sms)) != CTC_OK) return rc;
   const int grid = std::min(tb.C, num_sms);
   TcArgs a;
   a.tb = tb;
@@ -953,25 +959,17 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   a.order = w.order;
   a.tile_counter = w.counter;
   a.trace = nullptr;
+  a.wait_cycles = mol->wait_cycles > 0 ? (long long)mol->wait_cycles : kWaitCycles;
   // CTC_TC_TRACE=1: per-CTA cycle counters of the kernel's roles, summarised
   // on stderr after each launch (synchronises the stream; diagnostics only)
   static const bool trace_on = std::getenv("CTC_TC_TRACE") != nullptr;
   if (trace_on) CTC_CUDA_TRY(cudaMallocAsync((void**)&a.trace, sizeof(long long) * 8 * grid, st));
-  static bool attr[2] = {false, false};
+  if ((rc = ensure_smem_attr(plan.nqa == 4 ? (const void*)tc_tile_kernel<4> : (const void*)tc_tile_kernel<1>,
+                             kSmemTc)) != CTC_OK)
+    return rc;
   ProfScope ps(mol, 0, st);
-  if (plan.nqa == 4) {
-    if (!attr[1]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(tc_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc));
-      attr[1] = true;
-    }
-    tc_tile_kernel<4><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
-  } else {
-    if (!attr[0]) {
-      CTC_CUDA_TRY(cudaFuncSetAttribute(tc_tile_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemTc));
-      attr[0] = true;
-    }
-    tc_tile_kernel<1><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
-  }
+  if (plan.nqa == 4) tc_tile_kernel<4><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
+  else tc_tile_kernel<1><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
   CTC_CUDA_TRY(cudaGetLastError());
   if (trace_on) {
     std::vector<long long> tr((size_t)8 * grid);

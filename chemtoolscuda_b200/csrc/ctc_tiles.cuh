@@ -18,12 +18,11 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include "ctc_internal.h"
+#include "ctc_finalize.cuh"
 
 namespace ctc {
 
 namespace {
-
-constexpr double kPi = 3.14159265358979323846;
 
 __device__ __forceinline__ int ncomp_of_type_dev(int type) {
   switch (type) {
@@ -36,58 +35,6 @@ __device__ __forceinline__ int ncomp_of_type_dev(int type) {
     case 6: return 15;
     default: return 9;
   }
-}
-
-// Per-point partial sums produced by the contraction epilogues:
-//   s[0] rho, s[1..3] sum G0 d_k phi, s[4..9] Hb_ij = sum G0 d_i d_j phi,
-//   s[10..15] Ha_ij = sum Gi d_j phi  (ij = xx xy xz yy yz zz)
-__device__ __forceinline__ void finalize_point(const double* s, int nqa, int nq_ao,
-                                               const ctc_outputs& o, int64_t idx,
-                                               const ctc_params& prm) {
-  const double rho = s[0];
-  const double g0 = 2.0 * s[1], g1 = 2.0 * s[2], g2 = 2.0 * s[3];
-  double H[6] = {0, 0, 0, 0, 0, 0};
-  double tau = 0.0;
-  if (nqa == 4) {
-    for (int i = 0; i < 6; ++i) H[i] = 2.0 * (s[10 + i] + (nq_ao == 10 ? s[4 + i] : 0.0));
-    tau = 0.5 * (s[10] + s[13] + s[15]);
-  }
-  const double lap = H[0] + H[3] + H[5];
-  if (o.rho) o.rho[idx] = rho;
-  if (o.grad) {
-    o.grad[3 * idx] = g0;
-    o.grad[3 * idx + 1] = g1;
-    o.grad[3 * idx + 2] = g2;
-  }
-  if (o.hess) {
-    double* h = o.hess + 9 * idx;
-    h[0] = H[0]; h[1] = H[1]; h[2] = H[2];
-    h[3] = H[1]; h[4] = H[3]; h[5] = H[4];
-    h[6] = H[2]; h[7] = H[4]; h[8] = H[5];
-  }
-  if (o.lap) o.lap[idx] = lap;
-  if (o.tau_pd) o.tau_pd[idx] = tau;
-  if (o.tau_alpha) o.tau_alpha[idx] = tau + prm.alpha * lap;
-  const double gsq = g0 * g0 + g1 * g1 + g2 * g2;
-  if (o.rdg) {
-    // s = 1/(2 (3 pi^2)^(1/3)) |grad rho| / rho^(4/3), ratio set to 1e-20 where
-    // rho^(4/3) <= 1e-20 (src/evaluate_densbased.cu:44-89, src/cuda_utils.cu:71-84)
-    const double pref = 0.5 / cbrt(3.0 * kPi * kPi);
-    const double d43 = pow(rho, 4.0 / 3.0);
-    const double q = d43 > 1e-20 ? sqrt(gsq) / d43 : 1e-20;
-    o.rdg[idx] = pref * q;
-  }
-  if (o.shannon) o.shannon[idx] = rho * log(rho);
-  double w = 0.0, tf = 0.0;
-  if (o.weizsacker || o.gge) {
-    const double den = 8.0 * rho;
-    w = den > 1e-20 ? gsq / den : 1e-20;
-  }
-  if (o.thomas_fermi || o.gge) tf = 0.3 * pow(3.0 * kPi * kPi, 2.0 / 3.0) * pow(rho, 5.0 / 3.0);
-  if (o.weizsacker) o.weizsacker[idx] = w;
-  if (o.thomas_fermi) o.thomas_fermi[idx] = tf;
-  if (o.gge) o.gge[idx] = tf + prm.gge_a * w + prm.gge_b * lap;
-  if (o.general_ked) o.general_ked[idx] = tau + 0.25 * (prm.ked_a - 1.0) * lap;
 }
 
 // ------------------------------------------------------------------ tiles
@@ -103,6 +50,12 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   return v;
 }
 
+// 30-bit Morton key of each point; a point with a non-finite coordinate gets
+// kNonFiniteKey, so the sort puts such points after every finite one and they
+// share tiles only with each other (and at most one tile's finite points).
+constexpr uint32_t kNonFiniteKey = 1u << 30;
+constexpr int kMortonSortBits = 31;
+
 __global__ void morton_kernel(const double* __restrict__ pts, int64_t n, double lox, double loy,
                               double loz, double inv_cell, uint32_t* keys, int32_t* vals) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -112,8 +65,10 @@ __global__ void morton_kernel(const double* __restrict__ pts, int64_t n, double 
     c = c < 0.0 ? 0.0 : (c > 1023.0 ? 1023.0 : c);
     return (uint32_t)c;
   };
-  keys[i] = spread10(q(pts[3 * i], lox)) | (spread10(q(pts[3 * i + 1], loy)) << 1) |
-            (spread10(q(pts[3 * i + 2], loz)) << 2);
+  const double x = pts[3 * i], y = pts[3 * i + 1], z = pts[3 * i + 2];
+  keys[i] = isfinite(x) && isfinite(y) && isfinite(z)
+                ? spread10(q(x, lox)) | (spread10(q(y, loy)) << 1) | (spread10(q(z, loz)) << 2)
+                : kNonFiniteKey;
   vals[i] = (int32_t)i;
 }
 
@@ -166,10 +121,21 @@ __global__ void __launch_bounds__(kTileThreads)
   const int t = blockIdx.x, TP = tb.TP;
   const double* xyz = tb.xyz + (int64_t)t * TP * 3;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // centre = mean of the tile's points (padding repeats a real point)
+  // centre = mean of the tile's finite points (padding repeats a real point;
+  // a point with a non-finite coordinate gets NaN outputs and must not move
+  // the sphere of its tile mates)
+  __shared__ int s_nfin;
+  if (threadIdx.x == 0) s_nfin = 0;
+  __syncthreads();
   double c[3] = {0, 0, 0};
+  int nfin = 0;
   for (int j = threadIdx.x; j < TP; j += kTileThreads)
-    for (int d = 0; d < 3; ++d) c[d] += xyz[3 * j + d];
+    if (finite_point(xyz + 3 * j)) {
+      ++nfin;
+      for (int d = 0; d < 3; ++d) c[d] += xyz[3 * j + d];
+    }
+  for (int o = 16; o > 0; o >>= 1) nfin += __shfl_xor_sync(0xffffffffu, nfin, o);
+  if (lane == 0 && nfin) atomicAdd(&s_nfin, nfin);
   for (int d = 0; d < 3; ++d) {
     for (int o = 16; o > 0; o >>= 1) c[d] += __shfl_xor_sync(0xffffffffu, c[d], o);
     if (lane == 0) red[d][warp] = c[d];
@@ -178,11 +144,12 @@ __global__ void __launch_bounds__(kTileThreads)
   if (threadIdx.x < 3) {
     double acc = 0;
     for (int w = 0; w < kTileThreads / 32; ++w) acc += red[threadIdx.x][w];
-    sctr[threadIdx.x] = acc / TP;
+    sctr[threadIdx.x] = s_nfin ? acc / s_nfin : 0.0;
   }
   __syncthreads();
   double r2 = 0.0;
   for (int j = threadIdx.x; j < TP; j += kTileThreads) {
+    if (!finite_point(xyz + 3 * j)) continue;
     const double dx = xyz[3 * j] - sctr[0], dy = xyz[3 * j + 1] - sctr[1], dz = xyz[3 * j + 2] - sctr[2];
     r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
   }
@@ -192,7 +159,8 @@ __global__ void __launch_bounds__(kTileThreads)
   if (threadIdx.x == 0) {
     double m = 0;
     for (int w = 0; w < kTileThreads / 32; ++w) m = fmax(m, red[0][w]);
-    srad = sqrt(m) * (1.0 + 1e-12) + 1e-9;
+    // a tile without a finite point keeps no segment (radius -1)
+    srad = s_nfin ? sqrt(m) * (1.0 + 1e-12) + 1e-9 : -1e300;
     base_s = 0;
     base_k = 0;
   }
@@ -519,7 +487,9 @@ __global__ void __launch_bounds__(kThreads)
   for (int i = 0; i < NS; ++i) red[(esub * NS + i) * PTS + epl] = acc_s[i];
   __syncthreads();
   const int64_t oidx = tb.out[(int64_t)t * PTS + epl];
-  if (esub == 0 && oidx >= 0) {
+  if (esub == 0 && oidx >= 0 && !finite_point(tb.xyz + 3 * ((int64_t)t * PTS + epl))) {
+    nan_point(out, oidx);
+  } else if (esub == 0 && oidx >= 0) {
     double s[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
@@ -637,7 +607,8 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     }
     size_t tmp_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 30, st);
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0,
+                                    kMortonSortBits, st);
     const size_t need = 4 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
     if ((rc = mol->ws_part.ensure(need, st)) != CTC_OK) return rc;
     Carve cv{(char*)mol->ws_part.p};
@@ -650,7 +621,7 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
                                                                 1024.0 / ext, k_in, v_in);
     CTC_CUDA_TRY(cudaGetLastError());
     CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
-                                                 30, st));
+                                                 kMortonSortBits, st));
     mol->host_launches += 2;
   }
   for (int64_t t0 = 0; t0 < ntiles; t0 += C) {

@@ -4,13 +4,22 @@
  * point is extern "C", takes plain pointers and sizes, and returns 0 on
  * success or a negative CTC_ERR_* code; ctc_last_error() then describes the
  * failure (per calling thread).  Nothing here allocates device memory that
- * outlives the molecule handle, and no call keeps global device state: each
- * handle owns its device copy of the basis and density matrix.
+ * outlives the molecule handle: each handle owns its device copy of the basis
+ * and density matrix and its scratch.  The library keeps, per process, only
+ * which kernels have been configured on which device (their shared-memory
+ * limits, set once per device) and the no-allocation entry point's fixed
+ * array (ctc_eval_local_noalloc).
  *
  * Device-pointer entry points are stream-ordered on the stream passed in
- * (NULL = legacy default stream) and return before the work finishes.  The
+ * (NULL = legacy default stream) and return before the work finishes; they
+ * do not synchronise.  A failure that a kernel detects on the device (a
+ * bounded wait of the tensor-core pipeline running out) is recorded in the
+ * molecule's status word and reported as CTC_ERR_DEVICE by the next call on
+ * that molecule whose copy of the word has landed, or at once by
+ * ctc_molecule_sync_status.  Use one stream at a time per molecule.  The
  * *_host variants take host pointers, copy inputs and outputs themselves and
- * return after the results are in host memory.
+ * return after the results are in host memory (and report device failures
+ * of their own kernels).
  *
  * Layouts: points are row-major (N, 3) doubles; gradients (N, 3); Hessians
  * (N, 3, 3); scalar descriptors (N,).  AO functions follow the reference's
@@ -241,6 +250,21 @@ int ctc_molecule_get_stats(ctc_molecule* mol, double* stats /* [8] */);
 int ctc_molecule_reset_stats(ctc_molecule* mol);
 /* Time the contraction and AO kernels with CUDA events on their stream. */
 int ctc_molecule_set_profiling(ctc_molecule* mol, int32_t on);
+
+/* Wait for the stream, then report a failure any kernel of an earlier call on
+ * this molecule recorded on the device: CTC_ERR_DEVICE with the cause in
+ * ctc_last_error(), or CTC_OK.  Reporting clears the record, and the molecule
+ * stays usable.  The reference has no such path: its drivers turn a
+ * cudaError_t into a C++ exception (include/cuda_utils.cuh:55-60). */
+int ctc_molecule_sync_status(ctc_molecule* mol, void* stream);
+
+/* Limit, in SM clock cycles, of every wait in the tensor-core pipeline
+ * (0 = the default of 4e9 cycles, about 2 s).  A kernel whose wait runs out
+ * stops issuing work, waits for its own copies in flight, frees its tensor
+ * memory, records CTC_ERR_DEVICE in the status word and returns; the
+ * molecule stays usable.  A short limit makes the waits run out on purpose
+ * (tests of that path); no counterpart in the reference. */
+int ctc_molecule_set_wait_limit(ctc_molecule* mol, int64_t cycles);
 
 /* ---- misc ---------------------------------------------------------------------------------- */
 const char* ctc_last_error(void);

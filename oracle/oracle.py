@@ -92,22 +92,48 @@ def eval_ao(flat: dict, points: np.ndarray, deriv: int = 0, nthreads: int = 0) -
 
 
 LOCAL_KEYS = ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon")
+# Pointwise kinetic-energy densities formed from the C oracle's rho, grad rho,
+# lap rho and tau_PD (src/evaluate_densbased.cu:91-208):
+#   weizsacker   |grad rho|^2 / (8 rho), set to 1e-20 where 8 rho <= 1e-20
+#                (divide_inplace with mask 1e-20, :129-131, src/cuda_utils.cu:71-84)
+#   thomas_fermi 0.3 (3 pi^2)^(2/3) rho^(5/3)                           (:159-163)
+#   gge          thomas_fermi + a weizsacker + b lap                   (:173-191)
+#   general_ked  tau_PD + (a - 1)/4 lap                                (:195-208)
+DERIVED_KEYS = ("weizsacker", "thomas_fermi", "gge", "general_ked")
+ALL_KEYS = LOCAL_KEYS + DERIVED_KEYS
 
 
 def eval_local(flat: dict, D: np.ndarray, points: np.ndarray, alpha: float = 0.5,
-               keys=LOCAL_KEYS, nthreads: int = 0) -> dict:
+               keys=LOCAL_KEYS, nthreads: int = 0, gge_ab=(1 / 9, 1 / 6),
+               ked_a: float = 1.0) -> dict:
+    """Local descriptors at points; keys may name any of ALL_KEYS."""
     b = _Basis(flat)
     pts = np.ascontiguousarray(points, np.float64)
     Dm = np.ascontiguousarray(D, np.float64)
     n = len(pts)
+    keys = tuple(keys)
+    derived = [k for k in keys if k in DERIVED_KEYS]
+    need = set(k for k in keys if k in LOCAL_KEYS)
+    if derived:
+        need |= {"rho", "grad", "lap", "tau_pd"}
     shapes = dict(rho=(n,), grad=(n, 3), hess=(n, 3, 3), lap=(n,), tau_pd=(n,), tau_alpha=(n,),
                   rdg=(n,), shannon=(n,))
-    out = {k: np.zeros(shapes[k]) for k in keys}
+    out = {k: np.zeros(shapes[k]) for k in LOCAL_KEYS if k in need}
     rc = lib().ctco_eval_local(b.ptr, _p(Dm), Dm.shape[0], _p(pts), n, float(alpha),
                                *[_p(out.get(k)) for k in LOCAL_KEYS], nthreads)
     if rc != 0:
         raise ValueError("oracle: basis size does not match D")
-    return out
+    if derived:
+        rho, lap, tau = out["rho"], out["lap"], out["tau_pd"]
+        g2 = (out["grad"] ** 2).sum(1)
+        den = 8.0 * rho
+        w = np.where(den > 1e-20, g2 / np.where(den > 1e-20, den, 1.0), 1e-20)
+        with np.errstate(invalid="ignore"):  # pow of a negative rho is NaN, as in the reference
+            tf = 0.3 * (3.0 * np.pi ** 2) ** (2.0 / 3.0) * np.power(rho, 5.0 / 3.0)
+        extra = dict(weizsacker=w, thomas_fermi=tf, gge=tf + gge_ab[0] * w + gge_ab[1] * lap,
+                     general_ked=tau + 0.25 * (ked_a - 1.0) * lap)
+        out.update({k: extra[k] for k in derived})
+    return {k: out[k] for k in keys}
 
 
 def eval_esp(flat: dict, D: np.ndarray, coords: np.ndarray, charges: np.ndarray,

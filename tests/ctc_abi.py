@@ -81,6 +81,8 @@ def lib():
         L.ctc_molden_load.argtypes = [C.c_char_p, vp]
         L.ctc_wfn_load.argtypes = [C.c_char_p, vp]
         L.ctc_molecule_create_from_file.argtypes = [C.c_char_p, vp]
+        L.ctc_molecule_sync_status.argtypes = [vp, vp]
+        L.ctc_molecule_set_wait_limit.argtypes = [vp, i64]
     return _lib
 
 
@@ -164,6 +166,13 @@ class Mol:
         self.h = h
         self.M = k["D"].shape[0]
 
+    def sync_status(self) -> int:
+        """ctc_molecule_sync_status on the legacy default stream: its return code."""
+        return lib().ctc_molecule_sync_status(self.h, None)
+
+    def set_wait_limit(self, cycles: int):
+        check(lib().ctc_molecule_set_wait_limit(self.h, int(cycles)), "ctc_molecule_set_wait_limit")
+
     def close(self):
         if self.h:
             lib().ctc_molecule_destroy(self.h)
@@ -204,7 +213,10 @@ class Mol:
         return {k: (a.reshape(n, 3) if k == "grad" else (a.reshape(n, 3, 3) if k == "hess" else a))
                 for k, a in outs.items()}
 
-    def eval_cubic(self, origin, axes, shape, keys=("rho",), precision=PREC_FP64):
+    def eval_cubic(self, origin, axes, shape, keys=("rho",), precision=PREC_FP64, params=None,
+                   index=None):
+        """Descriptors on the cubic grid; with index (flat grid indices) only those points are
+        copied back, reshaped like eval_local's outputs."""
         import torch
         n = int(np.prod(shape))
         outs = {k: torch.full((n * OUT_WIDTH[k],), float("nan"), dtype=torch.float64, device="cuda")
@@ -213,10 +225,20 @@ class Mol:
         org = np.ascontiguousarray(origin, np.float64)
         ax = np.ascontiguousarray(axes, np.float64)
         sh = np.ascontiguousarray(shape, np.int32)
+        p = None if params is None else C.byref(Params(*params))
         check(lib().ctc_eval_cubic(self.h, org.ctypes.data, ax.ctypes.data, sh.ctypes.data,
-                                   precision, None, C.byref(o), None), "ctc_eval_cubic")
+                                   precision, p, C.byref(o), None), "ctc_eval_cubic")
         torch.cuda.synchronize()
-        return {k: t.cpu().numpy() for k, t in outs.items()}
+        if index is None:
+            return {k: t.cpu().numpy() for k, t in outs.items()}
+        idx = torch.as_tensor(np.asarray(index, np.int64), device="cuda")
+        res = {}
+        for k, t in outs.items():
+            w = OUT_WIDTH[k]
+            a = t.view(n, w)[idx].cpu().numpy()
+            res[k] = a.reshape(-1, 3) if k == "grad" else (a.reshape(-1, 3, 3) if k == "hess" else a.ravel())
+        del outs
+        return res
 
     def eval_ao(self, points, deriv):
         import torch

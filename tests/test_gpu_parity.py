@@ -182,21 +182,54 @@ def _golden_mol(g):
     return flat, ctc_abi.Mol(flat, g["in_coords"], g["in_charges"], g["in_D"])
 
 
-@pytest.mark.parametrize("case", ["c1", "esp", "mixed"])
-def test_fp64_path_vs_reference_outputs(torch_cuda, case):
-    """Directly against what the reference's CUDA drivers returned."""
+REF_PAIRS = dict(rho="ref_density", grad="ref_gradient", hess="ref_hessian", lap="ref_laplacian",
+                 tau_pd="ref_tau_pd", tau_alpha="ref_tau_general", rdg="ref_rdg",
+                 shannon="ref_shannon", weizsacker="ref_weizsacker",
+                 thomas_fermi="ref_thomas_fermi", gge="ref_gge", general_ked="ref_general_ked")
+RATIO_KEYS = ("rdg", "shannon", "weizsacker", "thomas_fermi", "gge")
+
+
+def _vs_reference(case, precision, rtol):
+    """Every output slot against what the reference's CUDA drivers returned on the
+    same molecule and points: |x - x_ref| <= rtol * (sum of |terms|) where
+    rho >= 1e-12 and <= 1e-12 absolute where rho < 1e-12; the ratio-type outputs
+    where rho > 1e-10 (their reference values divide by rho)."""
     g = _golden(case)
     flat, m = _golden_mol(g)
     pts = g["in_points"]
-    got = m.eval_local(pts, ("rho", "grad", "hess", "lap", "tau_pd", "tau_alpha", "rdg", "shannon"),
-                       params=(float(g["meta_tau_alpha"]), 1 / 9, 1 / 6, 1.0))
-    oref = O.eval_local(flat, g["in_D"], pts, alpha=float(g["meta_tau_alpha"]))
-    sc = term_scales(flat, g["in_D"], pts, alpha=float(g["meta_tau_alpha"]), ref=oref)
-    pairs = dict(rho="ref_density", grad="ref_gradient", hess="ref_hessian", lap="ref_laplacian",
-                 tau_pd="ref_tau_pd", tau_alpha="ref_tau_general")
-    for k, rk in pairs.items():
-        if rk in g:
-            assert_close(f"{case}/{k} vs reference", got[k], g[rk], sc[k], 1e-9, atol=1e-13)
+    a = float(g["meta_tau_alpha"])
+    ga, gb = (float(x) for x in g["meta_gge_ab"])
+    ka = float(g["meta_general_ked_a"])
+    keys = tuple(k for k, rk in REF_PAIRS.items() if rk in g)
+    got = m.eval_local(pts, keys, precision, params=(a, ga, gb, ka))
+    oref = O.eval_local(flat, g["in_D"], pts, alpha=a, keys=keys, gge_ab=(ga, gb), ked_a=ka)
+    sc = term_scales(flat, g["in_D"], pts, alpha=a, gge=(ga, gb), ked_a=ka, ref=oref)
+    rho = g["ref_density"]
+    tiny = rho < 1e-12
+    for k in keys:
+        ref = g[REF_PAIRS[k]].reshape(got[k].shape)
+        if k in RATIO_KEYS:
+            assert_close(f"{case}/{k} vs reference", got[k], ref, sc[k], rtol, atol=1e-15,
+                         mask=rho > 1e-10)
+            continue
+        scale = np.where(tiny.reshape((-1,) + (1,) * (ref.ndim - 1)), 0.0, rtol * sc[k])
+        atol = np.where(tiny, 1e-12, 1e-15).reshape((-1,) + (1,) * (ref.ndim - 1))
+        assert_close(f"{case}/{k} vs reference", got[k], ref, scale + atol, 1.0)
+    return m, g
+
+
+@pytest.mark.parametrize("case", ["c1", "esp", "mixed"])
+def test_fp64_path_vs_reference_outputs(torch_cuda, case):
+    """Directly against what the reference's CUDA drivers returned: 1e-10 relative
+    (1e-12 absolute where rho < 1e-12), every output slot."""
+    m, g = _vs_reference(case, ctc_abi.PREC_FP64, 1e-10)
     if "ref_esp" in g:
-        e = m.eval_esp(pts)
-        assert_close(f"{case}/esp vs reference", e, g["ref_esp"], np.abs(g["ref_esp"]) + 1.0, 1e-8)
+        e = m.eval_esp(g["in_points"])
+        assert_close(f"{case}/esp vs reference", e, g["ref_esp"], np.abs(g["ref_esp"]), 1e-10)
+
+
+@pytest.mark.parametrize("case", ["c1", "esp", "mixed"])
+def test_tc_path_vs_reference_outputs(torch_cuda, case):
+    """The tensor-core split path against the reference's own outputs at its
+    stated 1e-8 (1e-12 absolute where rho < 1e-12), every output slot."""
+    _vs_reference(case, ctc_abi.PREC_TC, 1e-8)

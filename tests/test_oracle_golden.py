@@ -115,6 +115,26 @@ def test_pointwise_kinetic_energy_densities_match_reference(case):
                  sc["tau_pd"] + abs(ka - 1) / 4 * sc["lap"], 1e-10, 1e-14)
 
 
+@pytest.mark.parametrize("case", [c for c in CASES if c != "allshell"])
+def test_oracle_derived_keds_match_reference(case):
+    """The oracle's own W, TF, GGE and general KED (oracle.eval_local) against the
+    reference's compute_weizsacker_ked, compute_thomas_fermi_energy_density,
+    compute_ked_gradient_expansion_general and compute_general_ked outputs."""
+    g, flat = load(case)
+    pts, D = g["in_points"], g["in_D"]
+    a, b = (float(x) for x in g["meta_gge_ab"])
+    ka = float(g["meta_general_ked_a"])
+    keys = ("rho", "grad", "lap", "tau_pd") + O.DERIVED_KEYS
+    ref = O.eval_local(flat, D, pts, keys=keys, gge_ab=(a, b), ked_a=ka)
+    sc = term_scales(flat, D, pts, gge=(a, b), ked_a=ka, ref=dict(ref, rdg=np.ones_like(ref["rho"])))
+    live = ref["rho"] > 1e-10
+    for k, rk in (("weizsacker", "ref_weizsacker"), ("thomas_fermi", "ref_thomas_fermi"),
+                  ("gge", "ref_gge")):
+        assert_close(k, ref[k], g[rk], sc[k], 1e-10, 1e-14, mask=live)
+    assert_close("general_ked", ref["general_ked"], g["ref_general_ked"], sc["general_ked"], 1e-10,
+                 1e-14)
+
+
 @pytest.mark.parametrize("case", ["c1", "esp"])
 def test_esp_matches_reference(case):
     g, flat = load(case)
