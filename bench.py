@@ -12,10 +12,12 @@ epilogue).  Inputs are synthetic (seeded); there is no dataset.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision tc|fp64]
     python bench.py --impl reference ...   # the reference's own CUDA drivers
 
-Prints one JSON line.  For N > 1 run under torch.distributed.run: every rank
-evaluates its own full-size grid (an independent density matrix of the same
-molecule), so per-GPU work is fixed ("scaling": "weak") and nothing crosses
-GPUs except the barrier and the max-over-ranks timing reduction.
+Prints one JSON line.  For N > 1 run under torch.distributed.run: by default
+every rank evaluates its own full-size grid (an independent density matrix of
+the same molecule), so per-GPU work is fixed ("scaling": "weak"); with
+--mode strong the one 215^3 grid is split into x-slabs over the ranks
+("scaling": "strong").  Nothing crosses GPUs except the barrier and the
+max-over-ranks timing reduction.
 """
 from __future__ import annotations
 
@@ -285,15 +287,25 @@ def run_ours(args, ws, rank, local):
     import torch
     lib = load_lib()
     mol = S.make_molecule("c2", seed=0)
-    if rank > 0:
+    if rank > 0 and args.mode == "weak":
         # independent density matrix per rank (same molecule and grid structure)
         rng = np.random.default_rng(1000 + rank)
         mol.D = S.make_density_matrix(rng, mol.nbasis, 400)
     h = create(lib, mol)
     prec = 1 if args.precision == "tc" else 0
     check(lib, lib.ctc_molecule_prepare(h, prec), "prepare")
-    shape = tuple(args.shape)
-    origin, axes = S.cube_grid(mol, SPACING, shape)
+    grid_shape = tuple(args.shape)
+    origin, axes = S.cube_grid(mol, SPACING, grid_shape)
+    if args.mode == "strong":
+        # one grid, x-slabs over the ranks (chemtoolscuda_b200.sharding.slab_bounds):
+        # each rank evaluates planes [lo, hi) and keeps its outputs
+        base, extra = divmod(grid_shape[0], ws)
+        lo = rank * base + min(rank, extra)
+        hi = lo + base + (1 if rank < extra else 0)
+        origin = origin + lo * np.asarray(axes)[0]
+        shape = (hi - lo,) + grid_shape[1:]
+    else:
+        shape = grid_shape
     n = int(np.prod(shape))
     outs = {k: torch.empty(n * WIDTH[k], dtype=torch.float64, device="cuda") for k in KEYS}
     o = Outputs(**{k: outs[k].data_ptr() for k in KEYS})
@@ -325,7 +337,9 @@ def run_ours(args, ws, rank, local):
     ms_max = allreduce_max(ms, ws)
     st = stats(lib, h)
     clocks = clk.summary()
-    value = ws * n * args.steps / (ms_max * 1e-3)
+    # whole-job points: N full grids (weak) or the one grid (strong)
+    job_points = ws * n if args.mode == "weak" else int(np.prod(grid_shape))
+    value = job_points * args.steps / (ms_max * 1e-3)
 
     # dominant kernel, timed live with events on the launching stream (separate pass)
     check(lib, lib.ctc_molecule_reset_stats(h), "reset")
@@ -360,7 +374,8 @@ def run_ours(args, ws, rank, local):
                     "kernel_ms_per_step": kern_ms, "ao_kernel_ms_per_step": pst[7],
                     "traffic": profile_traffic("fp64_tile_kernel", pst[0] / max(pst[5], 1.0)),
                     "tiles_per_launch": pst[0] / max(pst[5], 1.0)}
-        result = dict(value=value, ms=ms_max / args.steps, stats=st, roof=roof, clocks=clocks, n=n)
+        result = dict(value=value, ms=ms_max / args.steps, stats=st, roof=roof, clocks=clocks, n=n,
+                      job_points=job_points)
 
     # FP64 form of the same step (the metric compares the two forms)
     fp64 = None
@@ -376,7 +391,7 @@ def run_ours(args, ws, rank, local):
         e1.record()
         torch.cuda.synchronize()
         fms = allreduce_max(e0.elapsed_time(e1), ws) / fsteps
-        fp64 = {"value": ws * n / (fms * 1e-3), "ms_per_step": fms, "steps": fsteps,
+        fp64 = {"value": job_points / (fms * 1e-3), "ms_per_step": fms, "steps": fsteps,
                 "_sample": _gather(outs, sample_idx)}
 
     # end to end through the C ABI with host buffers (copies inside the timed region)
@@ -393,7 +408,7 @@ def run_ours(args, ws, rank, local):
             check(lib, lib.ctc_eval_local_host(h, pts.ctypes.data, n, prec, C.byref(prm),
                                                C.byref(ho)), "e2e")
         el = allreduce_max(time.perf_counter() - t0, ws)
-        e2e = {"value": ws * n * ksteps / el, "unit": "grid points/s", "steps": ksteps,
+        e2e = {"value": job_points * ksteps / el, "unit": "grid points/s", "steps": ksteps,
                "h2d_bytes_per_step": int(pts.nbytes),
                "d2h_bytes_per_step": int(sum(v.nbytes for v in hout.values())),
                "api": "ctc_eval_local_host (C ABI, host buffers)"}
@@ -607,10 +622,11 @@ def run_workload(args):
 
     c1: 12-atom molecule (Cartesian up to d), 1e5 points uniform in the box + 4 bohr, rho only,
         FP64 form and tensor-core form.
-    c3: 60-atom molecule (up to d), atom-centred grid of 75 radial x 308 angular points per atom
+    c3: 60-atom molecule (up to d, ~800 functions), atom-centred grid of 75 radial x 308 angular points per atom
         with Becke weights (~1.4e6 points); one step = forward (rho, grad rho), the GGA functional
         L = sum w (c1 rho^4/3 + c2 |grad rho|^2 / rho^4/3) and its adjoint (dL/dD, dL/dR);
-        checked against central differences (h = 1e-5) on 20 symmetric D pairs and 4 atoms.
+        checked against central differences (h = 1e-5) on 20 symmetric D pairs and all 180
+        atom coordinates.
     c4: 1000-atom molecule (Cartesian up to g, D zeroed beyond 12 bohr), 368^3 cube at 0.25 bohr
         (4.98e7 points), rho + grad rho + lap rho on the tensor-core path.
     c5: 100-atom molecule (up to d), electrostatic potential on its four nested surfaces.
@@ -693,7 +709,7 @@ def run_workload(args):
                 an = gD[a, b] + (gD[b, a] if a != b else 0.0)
                 errD = max(errD, abs(an - fd))
             errR = 0.0
-            for A in range(4):
+            for A in range(len(mol.coords)):
                 for j in range(3):
                     Rp, Rn = R.detach().clone(), R.detach().clone()
                     Rp[A, j] += hfd
@@ -705,7 +721,7 @@ def run_workload(args):
                      "higher_is_better": True, "dtype": "f64",
                      "config": {"workload": "c3: 60 atoms (up to d), 75 x 308 points per atom, Becke weights",
                                 "nbasis": M, "points": n},
-                     "finite_differences": {"h": hfd, "D_pairs": 20, "atoms": 4,
+                     "finite_differences": {"h": hfd, "D_pairs": 20, "coordinates": 3 * len(mol.coords),
                                             "max_err_dLdD_rel_max": errD / max(np.abs(gD).max(), 1e-300),
                                             "max_err_dLdR_rel_max": errR / max(np.abs(gR).max(), 1e-300)}})
     elif w == "c4":
@@ -778,6 +794,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="tc", choices=["tc", "fp64"])
+    ap.add_argument("--mode", default="weak", choices=["weak", "strong"],
+                    help="weak: every rank its own full grid; strong: one grid split in x-slabs")
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -814,9 +832,12 @@ def main():
         line = {
             "metric": METRIC, "value": res["value"], "unit": "grid points/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "higher_is_better": True, "scaling": args.mode, "vs_baseline": None, "dtype": dtype,
             "data": "synthetic",
             "config": workload_config(args.shape, nbasis),
+            "sharding": ("replicas: every rank evaluates its own full grid (independent D)"
+                         if args.mode == "weak" else
+                         f"one grid in x-slabs over {ws} ranks, {res['n']} points on the slowest rank's slab"),
             "pipeline": {"precision": args.precision, "tiles_per_step": res["stats"][0] / args.steps,
                          "mean_compact_aos_per_tile": res["stats"][2] / max(res["stats"][0], 1)},
             "roofline": res["roof"], "cpu_baseline": cpu, "parity": parity, "e2e": e2e,

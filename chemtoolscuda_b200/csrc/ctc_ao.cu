@@ -208,18 +208,19 @@ __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __
 // [ktrue, kt) are zeroed.
 //
 // SLICE = 4 or 1 also produces the row exponents of the tensor-core split
-// operands of the tile (ctc_split.cuh): the rows are 32 points x {phi, d_x,
-// d_y, d_z phi} (SLICE = 4, row = q * 32 + point) or 128 points x phi
-// (SLICE = 1).  Every lane keeps the running maximum of its values while it
-// evaluates, so the exponents cost no second pass over the block;
-// slice_rows_kernel then writes the digit planes.
+// operands of the tile (ctc_split.cuh): the rows are the tile's points x {phi,
+// d_x, d_y, d_z phi} (SLICE = 4, blocks of 32 points x 4 quantities, TP <= 64)
+// or its points x phi (SLICE = 1, TP <= 256).  Every lane keeps the running
+// maximum of its values while it evaluates, so the exponents cost no second
+// pass over the block; slice_rows_kernel then writes the digit planes.
 template <int DERIV, int SLICE>
 __global__ void __launch_bounds__(kAoThreads, 3)
     ao_tile_kernel(const DevSeg* __restrict__ segs, int nseg, const double* __restrict__ alpha,
                    const double* __restrict__ coef, TileBatch tb, int32_t* __restrict__ eexp,
                    const int32_t* __restrict__ order) {
   // per-warp maxima of the high word of |value| per row, [warp][row]
-  __shared__ unsigned s_mx[SLICE ? kAoThreads / 32 : 1][SLICE ? kSplitRows : 1];
+  constexpr int kMaxRows = 256;
+  __shared__ unsigned s_mx[SLICE ? kAoThreads / 32 : 1][SLICE ? kMaxRows : 1];
   const int t = order ? order[blockIdx.x] : blockIdx.x;
   const int ns = tb.nsig[t], TP = tb.TP;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kAoThreads, 3)
     }
     if (SLICE == 4) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) s_mx[SLICE ? warp : 0][SLICE ? q * 32 + lane : 0] = mx[q];
+      for (int q = 0; q < 4; ++q) s_mx[SLICE ? warp : 0][SLICE ? (pg / 32) * 128 + q * 32 + lane : 0] = mx[q];
     } else if (SLICE == 1) {
       s_mx[SLICE ? warp : 0][SLICE ? j : 0] = mx[0];
     }
@@ -252,15 +253,17 @@ __global__ void __launch_bounds__(kAoThreads, 3)
   }
   if (SLICE != 0) {
     __syncthreads();  // row maxima of every warp are in shared memory
-    const int r = threadIdx.x;  // one row per thread (kAoThreads == kSplitRows)
-    unsigned m = 0u;
+    const int rows = split_tile_rows(TP, SLICE);
+    for (int r = threadIdx.x; r < rows; r += kAoThreads) {
+      unsigned m = 0u;
 #pragma unroll
-    for (int w = 0; w < kAoThreads / 32; ++w) m = max(m, s_mx[SLICE ? w : 0][SLICE ? r : 0]);
-    // |x| = 1.f 2^(E - 1023) < 2^(E - 1022) for the biased exponent E of the
-    // largest |x| (frexp's exponent); a row of zeros gets 0
-    const int E = (int)(m >> 20);
-    const int e = m == 0u ? 0 : E - 1022;
-    eexp[(int64_t)t * kSplitRows + r] = e < kMinScaleExponent ? kMinScaleExponent : e;
+      for (int w = 0; w < kAoThreads / 32; ++w) m = max(m, s_mx[SLICE ? w : 0][SLICE ? r : 0]);
+      // |x| = 1.f 2^(E - 1023) < 2^(E - 1022) for the biased exponent E of the
+      // largest |x| (frexp's exponent); a row of zeros gets 0
+      const int E = (int)(m >> 20);
+      const int e = m == 0u ? 0 : E - 1022;
+      eexp[(int64_t)t * rows + r] = e < kMinScaleExponent ? kMinScaleExponent : e;
+    }
   }
 }
 
@@ -282,19 +285,23 @@ __global__ void __launch_bounds__(kSliceThreads, 2)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t ld_q = (int64_t)TP * tb.Kcap;
   const double* A = tb.ao + (int64_t)t * tb.nq * ld_q;
-  int8_t* P = planes + (int64_t)t * kSplitPlanesA * kSplitRows * tb.Kcap;
-  const int nitem = (kSplitRows / 32) * (kt / 32);  // warp-sized items
+  const int rows = split_tile_rows(TP, nqa);
+  int8_t* P = planes + (int64_t)t * kSplitPlanesA * rows * tb.Kcap;
+  const int nitem = (rows / 32) * (kt / 32);  // warp-sized items
   for (int it = warp; it < nitem; it += kSliceThreads / 32) {
-    const int rg = it % (kSplitRows / 32), c = it / (kSplitRows / 32);
-    const int r = rg * 32 + lane;
-    const int q = nqa == 4 ? rg : 0;
-    const int p = nqa == 4 ? lane : r;
-    const double f = split_row_factor(eexp[(int64_t)t * kSplitRows + r], kFixedBitsA);
+    const int rg = it % (rows / 32), c = it / (rows / 32);
+    const int r = rg * 32 + lane;             // tile row
+    const int blk = r / kSplitRows;           // 128-row block of the row
+    const int q = nqa == 4 ? rg % 4 : 0;      // quantity
+    const int p = nqa == 4 ? blk * 32 + lane : r;  // point
+    const double f = split_row_factor(eexp[(int64_t)t * rows + r], kFixedBitsA);
     const double* col = A + q * ld_q + p + (int64_t)(c * 32) * TP;
     double v[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __ldg(col + (int64_t)i * TP);
-    write_row_digits32([&](int i) { return v[i]; }, f, P, r, tb.Kcap, c * 32);
+    write_row_digits32([&](int i) { return v[i]; }, f,
+                       P + (int64_t)blk * kSplitPlanesA * kSplitRows * tb.Kcap, r % kSplitRows,
+                       tb.Kcap, c * 32);
   }
 }
 
@@ -349,7 +356,7 @@ int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cud
 int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
                            int8_t* planes, int32_t* eexp, const int32_t* order, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
-  if (!(nqa == 4 && tb.TP == 32 && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
+  if (!(nqa == 4 && (tb.TP == 32 || tb.TP == 64) && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
     return fail(CTC_ERR_INVALID, "sliced AO tiles: unsupported row layout");
   if (planes == nullptr || eexp == nullptr)
     return fail(CTC_ERR_INVALID, "sliced AO tiles: null workspace");

@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "ctc_internal.h"
 
@@ -40,22 +42,78 @@ double** slot(ctc_outputs* o, int i) {
   return s[i];
 }
 
-struct PinnedBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  ~PinnedBuf() { if (p) cudaFreeHost(p); }
-  int ensure(size_t b) {
-    if (b <= bytes) return CTC_OK;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    bytes = 0;
-    if (cudaMallocHost(&p, b) != cudaSuccess) return fail(CTC_ERR_NOMEM, "pinned host allocation failed");
-    bytes = b;
-    return CTC_OK;
+// memcpy of large host buffers on several threads: one thread moves ~5-10
+// GB/s, and the host side of the host-buffer pipeline moves ~160 B per point.
+void par_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kSlice = (size_t)8 << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>({(size_t)8, (size_t)hw, (bytes + kSlice - 1) / kSlice});
+  if (nt <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
   }
-};
+  std::vector<std::thread> th;
+  const size_t part = (bytes + nt - 1) / nt;
+  for (size_t t = 1; t < nt; ++t) {
+    const size_t b0 = t * part, b1 = std::min(bytes, b0 + part);
+    if (b0 < b1) th.emplace_back([=] { std::memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0); });
+  }
+  std::memcpy(dst, src, std::min(bytes, part));
+  for (auto& x : th) x.join();
+}
 
 }  // namespace
+
+namespace ctc {
+
+int HostPipe::ensure(size_t slab_bytes) {
+  if (!cs) {
+    CTC_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CTC_CUDA_TRY(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+    CTC_CUDA_TRY(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      CTC_CUDA_TRY(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming));
+      CTC_CUDA_TRY(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming));
+      CTC_CUDA_TRY(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming));
+    }
+  }
+  if (slab_bytes <= bytes) return CTC_OK;
+  for (int b = 0; b < 2; ++b) {
+    if (pin[b]) cudaFreeHost(pin[b]);
+    if (dbuf[b]) cudaFree(dbuf[b]);
+    pin[b] = nullptr;
+    dbuf[b] = nullptr;
+  }
+  bytes = 0;
+  for (int b = 0; b < 2; ++b) {
+    if (cudaMallocHost(&pin[b], slab_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CTC_ERR_NOMEM, "ctc_eval_local_host: pinned host staging allocation failed");
+    }
+    if (cudaMalloc((void**)&dbuf[b], slab_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CTC_ERR_NOMEM, "ctc_eval_local_host: device staging allocation failed");
+    }
+  }
+  bytes = slab_bytes;
+  return CTC_OK;
+}
+
+void HostPipe::release() {
+  for (int b = 0; b < 2; ++b) {
+    if (pin[b]) cudaFreeHost(pin[b]);
+    if (dbuf[b]) cudaFree(dbuf[b]);
+    if (ev_in[b]) cudaEventDestroy(ev_in[b]);
+    if (ev_comp[b]) cudaEventDestroy(ev_comp[b]);
+    if (ev_out[b]) cudaEventDestroy(ev_out[b]);
+  }
+  if (cs) cudaStreamDestroy(cs);
+  if (h2d) cudaStreamDestroy(h2d);
+  if (d2h) cudaStreamDestroy(d2h);
+  *this = HostPipe();
+}
+
+}  // namespace ctc
 
 extern "C" {
 
@@ -116,10 +174,12 @@ int ctc_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const doub
 }
 
 // Host-buffer variants: slabs of points go host -> device, through the
-// device path and back.  Kernels run on one compute stream (the molecule's
+// device path and back.  Kernels run on the molecule's compute stream (its
 // scratch is not shared across streams); the host->device copy of slab k+1
 // and the device->host copy of slab k-1 run on two copy streams while slab k
-// computes, ordered by events.
+// computes, ordered by events, and the host thread moves slab k-1's results
+// out of pinned memory (several threads) meanwhile.  Streams, events and
+// staging belong to the molecule (HostPipe): created on the first call.
 int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, int32_t precision,
                         const ctc_params* params, const ctc_outputs* h_out) {
   if (!mol || !h_out || (n > 0 && !h_points)) return fail(CTC_ERR_INVALID, "ctc_eval_local_host: null argument");
@@ -129,37 +189,29 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
   int width = 3;
   for (int i = 0; i < 12; ++i)
     if (*slot(const_cast<ctc_outputs*>(h_out), i)) width += kWidth[i];
-  const int64_t slab = std::min<int64_t>(n, std::max<int64_t>(chunk_points(mol, plan_local(h_out).nq_ao), 1 << 18));
-  static thread_local PinnedBuf pin[2];
-  size_t slab_bytes = sizeof(double) * (size_t)slab * width;
-  cudaStream_t cs = 0, h2d = 0, d2h = 0;
-  cudaEvent_t ev_in[2] = {0, 0}, ev_comp[2] = {0, 0}, ev_out[2] = {0, 0};
-  double* dbuf[2] = {nullptr, nullptr};
-  int rc = CTC_OK;
+  // slabs of up to 2^20 points: large enough that the device pipeline's
+  // per-call costs (point sort, chunk tails) stay small, small enough that
+  // the two staging slabs stay a few hundred MB
+  const int64_t slab = std::min<int64_t>(n, (int64_t)1 << 20);
+  const size_t slab_bytes = sizeof(double) * (size_t)slab * width;
+  if (!mol->hostpipe) mol->hostpipe = new HostPipe();
+  HostPipe& hp = *mol->hostpipe;
+  int rc = hp.ensure(slab_bytes);
+  if (rc != CTC_OK) return rc;
+  cudaStream_t cs = hp.cs, h2d = hp.h2d, d2h = hp.d2h;
   auto cuda_ok = [&](cudaError_t e, const char* what) {
     if (e != cudaSuccess && rc == CTC_OK) rc = fail(CTC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     return rc == CTC_OK;
   };
-  cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
-  cuda_ok(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking), "stream");
-  cuda_ok(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking), "stream");
-  for (int b = 0; b < 2 && rc == CTC_OK; ++b) {
-    cuda_ok(cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming), "event");
-    cuda_ok(cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming), "event");
-    cuda_ok(cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming), "event");
-    if (rc == CTC_OK) rc = pin[b].ensure(slab_bytes);
-    if (rc == CTC_OK && cudaMalloc((void**)&dbuf[b], slab_bytes) != cudaSuccess)
-      rc = fail(CTC_ERR_NOMEM, "ctc_eval_local_host: device staging allocation failed");
-  }
   int64_t pending_off[2] = {-1, -1}, pending_n[2] = {0, 0};
   auto drain = [&](int b) {
     if (pending_off[b] < 0 || rc != CTC_OK) return;
-    if (!cuda_ok(cudaEventSynchronize(ev_out[b]), "ctc_eval_local_host: wait")) return;
-    const double* hb = (const double*)pin[b].p + 3 * (size_t)pending_n[b];
+    if (!cuda_ok(cudaEventSynchronize(hp.ev_out[b]), "ctc_eval_local_host: wait")) return;
+    const double* hb = (const double*)hp.pin[b] + 3 * (size_t)pending_n[b];
     for (int i = 0; i < 12; ++i) {
       double* dst = *slot(const_cast<ctc_outputs*>(h_out), i);
       if (!dst) continue;
-      std::memcpy(dst + kWidth[i] * pending_off[b], hb, sizeof(double) * kWidth[i] * pending_n[b]);
+      par_copy(dst + kWidth[i] * pending_off[b], hb, sizeof(double) * kWidth[i] * pending_n[b]);
       hb += kWidth[i] * pending_n[b];
     }
     pending_off[b] = -1;
@@ -169,12 +221,12 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
     const int64_t m = std::min(slab, n - off);
     drain(b);
     if (rc != CTC_OK) break;
-    double* hp = (double*)pin[b].p;
-    double* dp = dbuf[b];
-    std::memcpy(hp, h_points + 3 * off, sizeof(double) * 3 * m);
-    if (!cuda_ok(cudaMemcpyAsync(dp, hp, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, h2d), "H2D") ||
-        !cuda_ok(cudaEventRecord(ev_in[b], h2d), "event") ||
-        !cuda_ok(cudaStreamWaitEvent(cs, ev_in[b], 0), "event"))
+    double* hpin = (double*)hp.pin[b];
+    double* dp = hp.dbuf[b];
+    par_copy(hpin, h_points + 3 * off, sizeof(double) * 3 * m);
+    if (!cuda_ok(cudaMemcpyAsync(dp, hpin, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, h2d), "H2D") ||
+        !cuda_ok(cudaEventRecord(hp.ev_in[b], h2d), "event") ||
+        !cuda_ok(cudaStreamWaitEvent(cs, hp.ev_in[b], 0), "event"))
       break;
     ctc_outputs d{};
     double* cur = dp + 3 * m;
@@ -187,11 +239,11 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
     src.pts = dp;
     rc = eval_local(mol, src, m, precision, &prm, &d, cs);
     if (rc != CTC_OK) break;
-    if (!cuda_ok(cudaEventRecord(ev_comp[b], cs), "event") ||
-        !cuda_ok(cudaStreamWaitEvent(d2h, ev_comp[b], 0), "event") ||
-        !cuda_ok(cudaMemcpyAsync(hp + 3 * m, dp + 3 * m, sizeof(double) * (width - 3) * m,
+    if (!cuda_ok(cudaEventRecord(hp.ev_comp[b], cs), "event") ||
+        !cuda_ok(cudaStreamWaitEvent(d2h, hp.ev_comp[b], 0), "event") ||
+        !cuda_ok(cudaMemcpyAsync(hpin + 3 * m, dp + 3 * m, sizeof(double) * (width - 3) * m,
                                  cudaMemcpyDeviceToHost, d2h), "D2H") ||
-        !cuda_ok(cudaEventRecord(ev_out[b], d2h), "event"))
+        !cuda_ok(cudaEventRecord(hp.ev_out[b], d2h), "event"))
       break;
     pending_off[b] = off;
     pending_n[b] = m;
@@ -199,20 +251,12 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
   drain(b);
   drain(b ^ 1);
   // a device-side failure of the tensor-core kernels of this call
-  if (rc == CTC_OK && cs && precision == CTC_PREC_TC_SPLIT)
+  if (rc == CTC_OK && precision == CTC_PREC_TC_SPLIT)
     rc = check_status(mol, cs, "ctc_eval_local_host");
-  if (cs) cudaStreamSynchronize(cs);
-  if (h2d) cudaStreamSynchronize(h2d);
-  if (d2h) cudaStreamSynchronize(d2h);
-  for (int k = 0; k < 2; ++k) {
-    if (dbuf[k]) cudaFree(dbuf[k]);
-    if (ev_in[k]) cudaEventDestroy(ev_in[k]);
-    if (ev_comp[k]) cudaEventDestroy(ev_comp[k]);
-    if (ev_out[k]) cudaEventDestroy(ev_out[k]);
-  }
-  if (cs) cudaStreamDestroy(cs);
-  if (h2d) cudaStreamDestroy(h2d);
-  if (d2h) cudaStreamDestroy(d2h);
+  // leave nothing of this call in flight (also after an error)
+  cudaStreamSynchronize(cs);
+  cudaStreamSynchronize(h2d);
+  cudaStreamSynchronize(d2h);
   return rc;
 }
 

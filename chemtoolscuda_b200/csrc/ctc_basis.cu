@@ -443,6 +443,10 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   m->ws_sl.release();
   m->ws_part.release();
   m->ws_misc.release();
+  if (m->hostpipe) {
+    m->hostpipe->release();
+    delete m->hostpipe;
+  }
   delete m;
   return CTC_OK;
 }

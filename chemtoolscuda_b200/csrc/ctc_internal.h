@@ -96,6 +96,21 @@ struct Scratch {
 // ESP pair data built once per molecule (see ctc_esp.cu).
 struct EspTables;
 
+// Host-buffer pipeline of a molecule (ctc_eval_local_host): a compute stream,
+// two copy streams, their events, and two slabs of device and pinned host
+// staging.  Created on the first host-buffer call and kept with the handle,
+// so later calls create and allocate nothing.
+struct HostPipe {
+  cudaStream_t cs = nullptr, h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr},
+              ev_out[2] = {nullptr, nullptr};
+  void* pin[2] = {nullptr, nullptr};
+  double* dbuf[2] = {nullptr, nullptr};
+  size_t bytes = 0;  // of each staging buffer
+  int ensure(size_t slab_bytes);
+  void release();
+};
+
 // One chunk of point tiles of the screened local pipeline (device pointers).
 // A tile holds TP points; its significant segments, compacted, define the
 // tile's own K dimension (kt, padded to a multiple of 64).
@@ -158,6 +173,7 @@ struct ctc_molecule {
   ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc;
   ctc::EspTables* esp = nullptr;
   bool esp_valid = false;
+  ctc::HostPipe* hostpipe = nullptr;
 };
 
 namespace ctc {
@@ -193,8 +209,8 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st);
 // Workspace of the digit planes and row exponents of a chunk of tiles, and
 // the chunk's tile order (largest compact K first), computed here from tb.kt;
 // tc_local_tiles on the same batch uses all three.
-int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, cudaStream_t st, int8_t** planes,
-                       int32_t** eexp, const int32_t** order);
+int tc_slice_workspace(ctc_molecule* mol, const TileBatch& tb, int nqa, cudaStream_t st,
+                       int8_t** planes, int32_t** eexp, const int32_t** order);
 int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb,
                    const ctc_params* prm, const ctc_outputs* out, cudaStream_t st);
 

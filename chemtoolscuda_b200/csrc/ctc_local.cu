@@ -69,13 +69,17 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
     if (rc != CTC_OK) return rc;
     if ((rc = prepare_tc(mol, st)) != CTC_OK) return rc;
   }
-  const int TP = 128 / plan.nqa;
+  // points per tile: 128 rows of the contraction (32 points x 4 quantities or
+  // 128 points x phi); the tensor-core path pairs two 128-row blocks on one
+  // B operand, so its tiles of phi and grad phi rows hold 64 points
+  const int TP = (precision == CTC_PREC_TC_SPLIT && plan.nqa == 4) ? 64 : 128 / plan.nqa;
+  const int rows = TP * plan.nqa;
   // tensor-core path: the AO kernel also writes the int8 digit planes
   const std::function<int(const TileBatch&)> sliced_ao = [&](const TileBatch& tb) {
     int8_t* planes = nullptr;
     int32_t* eexp = nullptr;
     const int32_t* order = nullptr;
-    int r = tc_slice_workspace(mol, tb, st, &planes, &eexp, &order);
+    int r = tc_slice_workspace(mol, tb, plan.nqa, st, &planes, &eexp, &order);
     if (r != CTC_OK) return r;
     return launch_ao_tiles_sliced(mol, tb, plan.deriv, plan.nqa, planes, eexp, order, st);
   };
@@ -92,7 +96,7 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
         mol->host_launches += 1;
         return r;
       },
-      precision == CTC_PREC_TC_SPLIT ? &sliced_ao : nullptr);
+      precision == CTC_PREC_TC_SPLIT ? &sliced_ao : nullptr, rows);
   if (rc != CTC_OK) return rc;
   // the tensor-core kernels report bounded-wait timeouts through the status
   // word: its copy is enqueued here and read by a later call (no wait now)

@@ -21,7 +21,14 @@ namespace ctc {
 
 constexpr int kSplitPlanesD = 4;  // digit planes of D (B operand)
 constexpr int kSplitPlanesA = 5;  // digit planes of the tile rows (A operand)
-constexpr int kSplitRows = 128;   // rows of a tile operand (MMA M)
+constexpr int kSplitRows = 128;   // rows of one block of a tile operand (MMA M)
+
+// A tile of TP points with nqa row quantities (nqa = 4: phi and grad phi;
+// nqa = 1: phi) has nqa * TP operand rows, stored in blocks of 128 rows:
+// digit planes [tile][block][5][128][Kcap], row exponents [tile][rows].
+// With nqa = 4 point p's quantity q is row (p / 32) * 128 + q * 32 + p % 32,
+// so every block holds 32 points x 4 quantities; with nqa = 1 row = point.
+__host__ __device__ constexpr int split_tile_rows(int TP, int nqa) { return TP * nqa; }
 constexpr int kFixedBitsD = 30;   // |I| <= 2^30
 constexpr int kFixedBitsA = 38;   // |I| <= 2^38
 

@@ -537,8 +537,11 @@ size_t tile_bytes(const ctc_molecule* mol, int C, int TP) {
 // kernel launch when given), then compute(tb).
 inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, int nq, int deriv,
                      cudaStream_t st, const std::function<int(const TileBatch&)>& compute,
-                     const std::function<int(const TileBatch&)>* ao_launch = nullptr) {
+                     const std::function<int(const TileBatch&)>* ao_launch = nullptr,
+                     int rows = 128) {
+  // cubic-grid tiles: blocks of 2x4x4, 4x4x4 or 4x4x8 grid points
   int TX = 2, TY = 4, TZ = 4;
+  if (TP == 64) { TX = 4; TY = 4; TZ = 4; }
   if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
   int64_t ntiles, nbx = 0, nby = 0, nbz = 0;
   int nx = 0;
@@ -633,7 +636,7 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     else
       tile_gather_kernel<<<g, 256, 0, st>>>(src.pts, perm, n, t0, tb);
     CTC_CUDA_TRY(cudaGetLastError());
-    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, 128, mol->d_stats);
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, rows, mol->d_stats);
     CTC_CUDA_TRY(cudaGetLastError());
     {
       ProfScope ps(mol, 1, st);

@@ -239,6 +239,19 @@ class Molecule {
     py::gil_scoped_release rel;
     check(ctc_eval_local(h_, (const double*)pts, n, pr, &p, &o, (void*)stream), "eval_local_device");
   }
+  void cubic_device(const arr& origin, const arr& axes, const iarr& shape, const std::string& prec,
+                    py::dict ptrs, double alpha, double gge_a, double gge_b, double ked_a,
+                    uintptr_t stream) {
+    if (origin.size() != 3 || axes.size() != 9 || shape.size() != 3)
+      throw py::value_error("origin (3), axes (3, 3) and shape (3) expected");
+    ctc_outputs o{};
+    for (auto item : ptrs) *slot(o, key_index(item.first.cast<std::string>())) = (double*)item.second.cast<uintptr_t>();
+    ctc_params p{alpha, gge_a, gge_b, ked_a};
+    int pr = parse_precision(prec);
+    py::gil_scoped_release rel;
+    check(ctc_eval_cubic(h_, origin.data(), axes.data(), shape.data(), pr, &p, &o, (void*)stream),
+          "eval_cubic_device");
+  }
   void esp_device(uintptr_t pts, int64_t n, uintptr_t out, uintptr_t stream) {
     py::gil_scoped_release rel;
     check(ctc_eval_esp(h_, (const double*)pts, n, (double*)out, (void*)stream), "eval_esp_device");
@@ -376,6 +389,10 @@ PYBIND11_MODULE(_chemtools_cuda, m) {
       .def("eval_local_device", &Molecule::local_device, py::arg("points_ptr"), py::arg("n"),
            py::arg("precision"), py::arg("ptrs"), py::arg("alpha") = 0.0, py::arg("gge_a") = 1.0 / 9.0,
            py::arg("gge_b") = 1.0 / 6.0, py::arg("ked_a") = 1.0, py::arg("stream") = 0)
+      .def("eval_cubic_device", &Molecule::cubic_device, py::arg("origin"), py::arg("axes"),
+           py::arg("shape"), py::arg("precision"), py::arg("ptrs"), py::arg("alpha") = 0.0,
+           py::arg("gge_a") = 1.0 / 9.0, py::arg("gge_b") = 1.0 / 6.0, py::arg("ked_a") = 1.0,
+           py::arg("stream") = 0)
       .def("eval_esp_device", &Molecule::esp_device, py::arg("points_ptr"), py::arg("n"),
            py::arg("out_ptr"), py::arg("stream") = 0)
       .def("eval_ao_device", &Molecule::ao_device, py::arg("points_ptr"), py::arg("n"),

@@ -114,3 +114,29 @@ def test_translational_sum_rule(torch_cuda):
     loc = m.eval_local(pts, ("grad", "hess"))
     expect = -(vr[:, None] * loc["grad"]).sum(0) - np.einsum("gij,gj->i", loc["hess"], vg)
     np.testing.assert_allclose(dR.sum(0), expect, rtol=1e-9, atol=1e-9 * np.abs(expect).max())
+
+
+@pytest.mark.parametrize("case", ["c1", "esp", "mixed"])
+def test_translational_sum_rule_vs_reference_outputs(torch_cuda, case):
+    """sum_A dL/dR_A = -sum_g (v_rho grad rho + H v_grad), the right-hand side
+    assembled from the reference's own gradient and Hessian outputs
+    (evaluate_electron_density_gradient, src/evaluate_gradient.cu:1197-1422;
+    evaluate_electron_density_hessian, src/evaluate_hessian.cu:1906-2307) on
+    the same molecule and points (golden vectors).  Every shell sits on an
+    atom, so moving all atoms together moves the density rigidly."""
+    import os
+    g = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"{case}.npz")))
+    flat = {k[3:]: g[k] for k in ("in_centers", "in_shell_atom", "in_nprim", "in_nseg",
+                                   "in_angmoms", "in_exps", "in_coeffs")}
+    pts = g["in_points"]
+    n = len(pts)
+    rng = np.random.default_rng(11)
+    vr = rng.standard_normal(n)
+    vg = rng.standard_normal((n, 3))
+    m = ctc_abi.Mol(flat, g["in_coords"], g["in_charges"], g["in_D"])
+    _, dR = m.adjoint(pts, vr, vg, want_D=False)
+    grad = g["ref_gradient"].reshape(n, 3)
+    hess = g["ref_hessian"].reshape(n, 3, 3)
+    expect = -(vr[:, None] * grad).sum(0) - np.einsum("gij,gj->i", hess, vg)
+    scale = (np.abs(vr)[:, None] * np.abs(grad)).sum(0) + np.einsum("gij,gj->i", np.abs(hess), np.abs(vg))
+    np.testing.assert_array_less(np.abs(dR.sum(0) - expect), 1e-10 * scale + 1e-14)

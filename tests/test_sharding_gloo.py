@@ -5,7 +5,11 @@ on CPU: two gloo ranks on 127.0.0.1.
 * max_over_ranks returns the largest per-rank value on every rank;
 * sharded_adjoint: each rank runs the adjoint of its own slice (here the FP64
   oracle stands in for the GPU kernels) and the all-reduced dL/dD and dL/dR
-  equal the single-process result to rounding.
+  equal the single-process result to rounding;
+* sharded_cubic / sharded_points: each rank evaluates its x-slab of one cubic
+  grid (or its slice of the points) -- the oracle again standing in for the
+  GPU -- and the slabs, in place or gathered, equal the whole grid evaluated
+  in one process.
 """
 import multiprocessing as mp
 import os
@@ -67,6 +71,107 @@ def _worker(rank, port, q):
         q.put((rank, mx, dD.numpy(), dR.numpy(), None))
     except Exception as e:  # report to the parent instead of hanging it
         q.put((rank, None, None, None, repr(e)))
+
+
+GRID_SHAPE = (7, 5, 6)   # 7 x-planes: ragged over 2 ranks
+
+
+def _grid(mol):
+    from chemtoolscuda_b200 import synthetic as S
+    return S.cube_grid(mol, 0.45, GRID_SHAPE)
+
+
+def _oracle_cubic(mol, keys):
+    import torch
+    from chemtoolscuda_b200 import synthetic as S
+    from oracle import oracle as O
+
+    def f(origin, axes, shape):
+        pts = S.cube_points(origin, axes, shape)
+        r = O.eval_local(mol.flat(), mol.D, pts, keys=keys)
+        return {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in r.items()}
+
+    return f
+
+
+def _oracle_points(mol, keys):
+    import torch
+    from oracle import oracle as O
+
+    def f(points):
+        r = O.eval_local(mol.flat(), mol.D, points.numpy(), keys=keys)
+        return {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in r.items()}
+
+    return f
+
+
+def _forward_worker(rank, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from chemtoolscuda_b200.sharding import sharded_cubic, sharded_points
+    try:
+        os.environ["MASTER_ADDR"] = "127.0.0.1"
+        os.environ["MASTER_PORT"] = str(port)
+        dist.init_process_group("gloo", rank=rank, world_size=WORLD,
+                                timeout=datetime.timedelta(seconds=60))
+        mol, pts, _, _ = _case()
+        origin, axes = _grid(mol)
+        keys = ("rho", "grad")
+        lo, hi, own = sharded_cubic(origin, axes, GRID_SHAPE, evaluate=_oracle_cubic(mol, keys), keys=keys)
+        _, _, full = sharded_cubic(origin, axes, GRID_SHAPE, evaluate=_oracle_cubic(mol, keys),
+                                   keys=keys, gather=True)
+        plo, phi, pown = sharded_points(torch.from_numpy(pts), evaluate=_oracle_points(mol, keys), keys=keys)
+        _, _, pfull = sharded_points(torch.from_numpy(pts), evaluate=_oracle_points(mol, keys), keys=keys,
+                                     gather=True)
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, dict(lo=lo, hi=hi, own={k: v.numpy() for k, v in own.items()},
+                          full={k: v.numpy() for k, v in full.items()}, plo=plo, phi=phi,
+                          pown={k: v.numpy() for k, v in pown.items()},
+                          pfull={k: v.numpy() for k, v in pfull.items()}), None))
+    except Exception as e:  # report to the parent instead of hanging it
+        q.put((rank, None, repr(e)))
+
+
+def test_two_gloo_ranks_sharded_forward():
+    from chemtoolscuda_b200 import synthetic as S
+    from oracle import oracle as O
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_forward_worker, args=(r, port, q)) for r in range(WORLD)]
+    for p in procs:
+        p.start()
+    res = {}
+    try:
+        for _ in range(WORLD):
+            rank, r, err = q.get(timeout=240)
+            assert err is None, f"rank {rank}: {err}"
+            res[rank] = r
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    mol, pts, _, _ = _case()
+    origin, axes = _grid(mol)
+    keys = ("rho", "grad")
+    whole = O.eval_local(mol.flat(), mol.D, S.cube_points(origin, axes, GRID_SHAPE), keys=keys)
+    wp = O.eval_local(mol.flat(), mol.D, pts, keys=keys)
+    plane = GRID_SHAPE[1] * GRID_SHAPE[2]
+    covered = []
+    for rank in range(WORLD):
+        r = res[rank]
+        assert (r["lo"], r["hi"]) == shard_bounds(GRID_SHAPE[0], rank, WORLD)
+        covered.extend(range(r["lo"], r["hi"]))
+        for k in keys:
+            np.testing.assert_allclose(r["own"][k], whole[k][r["lo"] * plane:r["hi"] * plane],
+                                       rtol=1e-13, atol=1e-16)
+            np.testing.assert_allclose(r["full"][k], whole[k], rtol=1e-13, atol=1e-16)
+            np.testing.assert_allclose(r["pown"][k], wp[k][r["plo"]:r["phi"]], rtol=1e-13, atol=1e-16)
+            np.testing.assert_allclose(r["pfull"][k], wp[k], rtol=1e-13, atol=1e-16)
+    assert covered == list(range(GRID_SHAPE[0]))
 
 
 @pytest.mark.parametrize("n", [0, 1, 2, 7, 301, 1000])
