@@ -164,6 +164,11 @@ int ctc_eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d
   return eval_esp(mol, d_points, n, d_out, (cudaStream_t)stream);
 }
 
+int ctc_molecule_esp_info(ctc_molecule* mol, double* info) {
+  if (!mol || !info) return fail(CTC_ERR_INVALID, "ctc_molecule_esp_info: null argument");
+  return esp_info(mol, info);
+}
+
 int ctc_adjoint(ctc_molecule* mol, const double* d_points, int64_t n, const double* d_v_rho,
                 const double* d_v_grad, double* d_dLdD, double* d_dLdR, void* stream) {
   if (!mol || (n > 0 && (!d_points || !d_v_rho)))

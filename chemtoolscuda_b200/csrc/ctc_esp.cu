@@ -87,6 +87,10 @@ struct EspTables {
   double* d_atoms = nullptr;  // x y z Z per atom
   int npairs = 0, nbatch = 0, natom = 0;
   size_t nh = 0;
+  // algorithmic FP64 work per point: sum over the kept pairs of
+  // 2 n_tuv(L) (contraction) + 2 n_R(L) (R recursion) + 10 (L + 1) (Boys)
+  double flops_per_point = 0.0;
+  double mean_L = 0.0;
 };
 
 namespace {
@@ -432,6 +436,14 @@ static int build_esp(ctc_molecule* mol) {
   }
   EspTables* e = new EspTables();
   mol->esp = e;
+  for (const EspBatch& bt : batches) {
+    int nR = 0;
+    for (int j = 0; j <= bt.L; ++j) nR += ntuv(j);
+    const int np = bt.b1 - bt.b0;
+    e->flops_per_point += (double)np * (2.0 * ntuv(bt.L) + 2.0 * nR + 10.0 * (bt.L + 1));
+    e->mean_L += (double)np * bt.L;
+  }
+  if (!pairs.empty()) e->mean_L /= (double)pairs.size();
   e->npairs = (int)pairs.size();
   e->nbatch = (int)batches.size();
   e->natom = mol->natom;
@@ -455,6 +467,18 @@ static int build_esp(ctc_molecule* mol) {
   if (std::getenv("CTC_LOG"))
     std::fprintf(stderr, "[ctc] esp tables: %d primitive pairs, %d batches, %zu Hermite coefficients\n",
                  e->npairs, e->nbatch, e->nh);
+  return CTC_OK;
+}
+
+int esp_info(ctc_molecule* mol, double* info) {
+  if (!mol->esp_valid) {
+    int rc = build_esp(mol);
+    if (rc != CTC_OK) return rc;
+  }
+  info[0] = mol->esp->npairs;
+  info[1] = mol->esp->flops_per_point;
+  info[2] = (double)mol->esp->nh;
+  info[3] = mol->esp->mean_L;
   return CTC_OK;
 }
 

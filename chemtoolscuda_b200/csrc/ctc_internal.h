@@ -223,6 +223,8 @@ struct LocalSums;
 
 // ---- ESP (ctc_esp.cu) ----
 int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, cudaStream_t st);
+// [0] kept primitive pairs, [1] FP64 flops per point, [2] Hermite coefficients, [3] mean L
+int esp_info(ctc_molecule* mol, double* info);
 void destroy_esp(ctc_molecule* mol);
 
 // ---- adjoint (ctc_adjoint.cu) ----

@@ -228,6 +228,14 @@ int ctc_eval_esp(ctc_molecule* mol, const double* d_points, int64_t npoints, dou
                  void* stream);
 int ctc_eval_esp_host(ctc_molecule* mol, const double* h_points, int64_t npoints, double* h_out);
 
+/* Work of the ESP evaluation (no counterpart in the reference; builds the
+ * molecule's pair tables if needed): info[0] primitive pairs kept after the
+ * point-independent screening, [1] algorithmic FP64 operations per point,
+ * sum over those pairs of 2 n_tuv(L) + 2 n_R(L) + 10 (L + 1) with
+ * n_tuv(L) = (L+1)(L+2)(L+3)/6 and n_R(L) = sum_{j<=L} n_tuv(j), [2] Hermite
+ * coefficients stored, [3] mean L = l_a + l_b of the kept pairs. */
+int ctc_molecule_esp_info(ctc_molecule* mol, double* info /* [4] */);
+
 /* ---- adjoint (no counterpart in the reference) --------------------------------------------- */
 
 /* Given v_rho = dL/drho (N) and v_grad = dL/d(grad rho) (N,3, may be NULL)

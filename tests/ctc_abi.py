@@ -83,6 +83,7 @@ def lib():
         L.ctc_molecule_create_from_file.argtypes = [C.c_char_p, vp]
         L.ctc_molecule_sync_status.argtypes = [vp, vp]
         L.ctc_molecule_set_wait_limit.argtypes = [vp, i64]
+        L.ctc_molecule_esp_info.argtypes = [vp, vp]
     return _lib
 
 

@@ -8,6 +8,7 @@ tests/test_hessian.cu, tests/test_laplacian.cu, tests/test_kinetic_density.cu,
 tests/test_electrostatic_potential.cu), here applied relative to the per-point
 sum of absolute terms (tests/helpers.py) and, for the reference's known
 defects, documented where they show up."""
+import glob
 import os
 
 import numpy as np
@@ -157,3 +158,30 @@ def test_cubic_grid_matches_reference(case):
     ref = O.eval_local(flat, g["in_D"], pts, keys=("rho",))
     sc = term_scales(flat, g["in_D"], pts)
     assert_close("cubic", ref["rho"], g["ref_cubic"].ravel(), sc["rho"], 1e-10, 1e-14)
+
+
+FIXTURES = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "fixtures", "*.npz")))
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_oracle_on_reference_fixture_molecules(path):
+    """The oracle against the reference's drivers on the reference's own
+    fixture molecules (tests/golden/fixtures, make_fixture_golden.py)."""
+    g = dict(np.load(path))
+    if "ref_density" not in g:
+        pytest.skip("reference outputs not generated")
+    flat = {k[3:]: g[k] for k in ("in_centers", "in_shell_atom", "in_nprim", "in_nseg",
+                                   "in_angmoms", "in_exps", "in_coeffs")}
+    pts, D = g["in_points"], g["in_D"]
+    a = float(g["meta_tau_alpha"])
+    ref = O.eval_local(flat, D, pts, alpha=a)
+    sc = term_scales(flat, D, pts, alpha=a, ref=ref)
+    pairs = dict(rho="ref_density", grad="ref_gradient", hess="ref_hessian", lap="ref_laplacian",
+                 tau_pd="ref_tau_pd", tau_alpha="ref_tau_general")
+    for k, rk in pairs.items():
+        assert_close(k, ref[k], g[rk].reshape(ref[k].shape), sc[k], 1e-10, 1e-14)
+    live = ref["rho"] > 1e-10
+    assert_close("rdg", ref["rdg"], g["ref_rdg"], sc["rdg"], 1e-10, 1e-14, mask=live)
+    if "ref_esp" in g:
+        e = O.eval_esp(flat, D, g["in_coords"], g["in_charges"], pts)
+        assert_close("esp", e, g["ref_esp"], np.abs(g["ref_esp"]), 1e-9)
