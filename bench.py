@@ -65,6 +65,19 @@ WORKLOAD = ("c2: 200-atom molecule (pure d/f, 2655 basis functions), 215^3 cubic
             "rho+grad+Hessian+lap+tau_PD+tau_alpha(0.5)+RDG")
 
 
+ESP_SUB_WORKLOAD = ("ESP on the leading atoms of the 100-atom ESP molecule that fit the reference's "
+                    "constant-memory basis (90 atoms, 1506 functions, D of 180 occupied columns), "
+                    "points on its four nested surfaces")
+
+
+def esp_submolecule():
+    """The sub-molecule both arms time the ESP on, and its surface points."""
+    full = S.make_molecule("c5", seed=0)
+    k = S.reference_esp_fit(full)
+    sub = S.submolecule(full, k, nocc=2 * k, seed=5)
+    return sub, S.esp_workload_points(sub, seed=0)
+
+
 def workload_config(shape, nbasis):
     """The config object both arms print, so the two lines describe one workload."""
     return {"workload": WORKLOAD, "nbasis": int(nbasis), "grid": list(shape),
@@ -449,6 +462,22 @@ def run_ours(args, ws, rank, local):
                "surface_points_total": int(len(sp)), "nbasis": mol5.nbasis, "atoms": 100,
                "ms": ems, "roofline": esp_roofline(lib, h5, m, ems, fp64_peak_tflops())}
         lib.ctc_molecule_destroy(h5)
+        # the sub-molecule the reference arm times its ESP on
+        sub, ssp = esp_submolecule()
+        hs = create(lib, sub)
+        ps = torch.as_tensor(np.ascontiguousarray(ssp), device="cuda")
+        os_ = torch.empty(len(ssp), dtype=torch.float64, device="cuda")
+        check(lib, lib.ctc_eval_esp(hs, ps.data_ptr(), len(ssp), os_.data_ptr(), stream), "esp")
+        torch.cuda.synchronize()
+        e0.record()
+        check(lib, lib.ctc_eval_esp(hs, ps.data_ptr(), len(ssp), os_.data_ptr(), stream), "esp")
+        e1.record()
+        torch.cuda.synchronize()
+        sms = e0.elapsed_time(e1)
+        esp["reference_submolecule"] = {"value": len(ssp) / (sms * 1e-3), "unit": "ESP points/s",
+                                        "points": int(len(ssp)), "atoms": len(sub.coords),
+                                        "nbasis": sub.nbasis, "workload": ESP_SUB_WORKLOAD}
+        lib.ctc_molecule_destroy(hs)
 
     # CPU baseline: the FP64 oracle on this host's cores, bounded sample of the same grid;
     # its outputs are also the checker of the parity block (GPU outputs at the same points)
@@ -566,6 +595,35 @@ def run_reference(args, ws, rank):
         step(samples[args.warmup + i])
     el = time.perf_counter() - t0
     value = n * args.steps / el
+
+    # ESP on the largest sub-molecule of the 100-atom ESP molecule that the
+    # reference's ESP accepts (its whole basis in constant memory), on a bounded
+    # sample of that sub-molecule's surface points
+    esp = None
+    if not args.no_esp:
+        sub, sp = esp_submolecule()
+        fs = sub.flat()
+        ks = [np.ascontiguousarray(fs[k]) for k in ("centers", "nprim", "nseg", "angmoms", "exps", "coeffs")]
+        sx, sq, sD = (np.ascontiguousarray(a) for a in (sub.coords, sub.charges, sub.D))
+        lib.ref_esp.argtypes = [vp, vp, i32, vp]
+        hs = lib.ref_create(len(fs["nprim"]), *[k.ctypes.data for k in ks], len(sx), sx.ctypes.data,
+                            sq.ctypes.data, sD.ctypes.data, sD.shape[0])
+        if not hs:
+            esp = {"unavailable": lib.ref_last_error().decode()}
+        else:
+            m = args.ref_esp_points
+            pe = np.ascontiguousarray(sp[np.random.default_rng(13).choice(len(sp), m + 4, replace=False)])
+            oe = np.empty(m + 4)
+            if lib.ref_esp(hs, pe[m:].ctypes.data, 4, oe[m:].ctypes.data) != 0:   # warm-up
+                raise RuntimeError(lib.ref_last_error().decode())
+            t0 = time.perf_counter()
+            if lib.ref_esp(hs, pe.ctypes.data, m, oe.ctypes.data) != 0:
+                raise RuntimeError(lib.ref_last_error().decode())
+            ee = time.perf_counter() - t0
+            esp = {"value": m / ee, "unit": "ESP points/s", "points": m, "atoms": len(sx),
+                   "nbasis": int(sD.shape[0]), "surface_points_total": int(len(sp)),
+                   "workload": ESP_SUB_WORKLOAD,
+                   "timing": "wall clock around compute_electrostatic_potential_over_points"}
     return {"metric": METRIC, "value": value, "unit": "grid points/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -586,7 +644,8 @@ def run_reference(args, ws, rank):
                                        "CUDA code (no CPU implementation): its own drivers built from "
                                        "its sources for sm_100a (oracle/_ref) run on this box's GPU"},
             "e2e": {"value": value, "unit": "grid points/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "esp": esp}
 
 
 # --------------------------------------------------------------------------- main
@@ -822,6 +881,8 @@ def main():
     ap.add_argument("--cpu-points", type=int, default=10000)
     ap.add_argument("--esp-points", type=int, default=0,
                     help="ESP leg points (0: the whole surface set of the 100-atom molecule)")
+    ap.add_argument("--ref-esp-points", type=int, default=48,
+                    help="reference arm: surface points of its ESP sample")
     ap.add_argument("--ref-points", type=int, default=0,
                     help="reference arm points per step (0: the largest batch its 32-bit indexing allows)")
     ap.add_argument("--workload", default=None, choices=["c1", "c3", "c4", "c5"],

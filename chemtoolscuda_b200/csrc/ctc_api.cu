@@ -256,8 +256,7 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
   drain(b);
   drain(b ^ 1);
   // a device-side failure of the tensor-core kernels of this call
-  if (rc == CTC_OK && precision == CTC_PREC_TC_SPLIT)
-    rc = check_status(mol, cs, "ctc_eval_local_host");
+  if (rc == CTC_OK) rc = check_status(mol, cs, "ctc_eval_local_host");
   // leave nothing of this call in flight (also after an error)
   cudaStreamSynchronize(cs);
   cudaStreamSynchronize(h2d);

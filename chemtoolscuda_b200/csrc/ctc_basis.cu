@@ -152,6 +152,9 @@ static std::string status_message(int32_t code) {
   if (code == 0x7101)
     return "a bounded wait of the tensor-core contraction ran out (status 0x7101); "
            "the call's outputs are incomplete";
+  if (code == 0x7201)
+    return "a tile's significant functions exceeded the workspace capacity (status 0x7201); "
+           "the call's outputs are incomplete";
   return "kernel status " + std::to_string(code);
 }
 
@@ -410,7 +413,7 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
 #undef ALLOC_COPY
   if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
       cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess ||
-      cudaMallocHost((void**)&m->h_status, sizeof(int32_t)) != cudaSuccess ||
+      cudaMallocHost((void**)&m->h_status, 4 * sizeof(int32_t)) != cudaSuccess ||
       cudaEventCreateWithFlags(&m->status_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaMalloc((void**)&m->d_stats, sizeof(double) * 8) != cudaSuccess ||
       cudaMemset(m->d_stats, 0, sizeof(double) * 8) != cudaSuccess) {
@@ -443,6 +446,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   m->ws_sl.release();
   m->ws_part.release();
   m->ws_misc.release();
+  m->ws_cap.release();
   if (m->hostpipe) {
     m->hostpipe->release();
     delete m->hostpipe;

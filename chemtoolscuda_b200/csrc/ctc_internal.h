@@ -156,7 +156,8 @@ struct ctc_molecule {
   double* d_Dscale = nullptr;
   bool dsl_valid = false;
   // status word written by kernels (sticky until reported), its pinned host
-  // copy, and the event recorded after the copy was enqueued
+  // copy ([0]; [1] receives the capacity pre-pass's count), and the event
+  // recorded after the copy was enqueued
   int32_t* d_status = nullptr;
   int32_t* h_status = nullptr;
   cudaEvent_t status_ev = nullptr;
@@ -170,7 +171,7 @@ struct ctc_molecule {
   bool prof = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[2];
   // scratch
-  ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc;
+  ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc, ws_cap;
   ctc::EspTables* esp = nullptr;
   bool esp_valid = false;
   ctc::HostPipe* hostpipe = nullptr;

@@ -63,11 +63,10 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
   if (!src.cubic && n > (int64_t)INT32_MAX)
     return fail(CTC_ERR_INVALID, "eval_local: at most 2^31-1 points per call");
   const LocalPlan plan = plan_local(out);
+  // a failure an earlier stream-ordered call recorded on the device
+  if (int rc = poll_status(mol, st); rc != CTC_OK) return rc;
   if (precision == CTC_PREC_TC_SPLIT) {
-    // a failure an earlier stream-ordered call recorded on the device
-    int rc = poll_status(mol, st);
-    if (rc != CTC_OK) return rc;
-    if ((rc = prepare_tc(mol, st)) != CTC_OK) return rc;
+    if (int rc = prepare_tc(mol, st); rc != CTC_OK) return rc;
   }
   // points per tile: 128 rows of the contraction (32 points x 4 quantities or
   // 128 points x phi); the tensor-core path pairs two 128-row blocks on one
@@ -98,10 +97,10 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
       },
       precision == CTC_PREC_TC_SPLIT ? &sliced_ao : nullptr, rows);
   if (rc != CTC_OK) return rc;
-  // the tensor-core kernels report bounded-wait timeouts through the status
-  // word: its copy is enqueued here and read by a later call (no wait now)
-  if (precision == CTC_PREC_TC_SPLIT) return post_status(mol, st);
-  return CTC_OK;
+  // kernels report failures (bounded-wait timeouts of the tensor-core
+  // kernels, a tile beyond the workspace capacity) through the status word:
+  // its copy is enqueued here and read by a later call (no wait now)
+  return post_status(mol, st);
 }
 
 }  // namespace ctc

@@ -132,7 +132,7 @@ int eval_local_noalloc(ctc_molecule* mol, const double* d_points, int64_t n, con
   const size_t ao_per_tile = sizeof(double) * (size_t)plan.nq_ao * TP * mol->Mpad;
   const size_t avail = kNoAllocScratchBytes - sort_end;
   auto chunk_bytes = [&](int64_t c) {
-    return tile_bytes(mol, (int)c, TP) + 256 + ao_per_tile * (size_t)c;
+    return tile_bytes(mol, (int)c, TP, mol->Mpad) + 256 + ao_per_tile * (size_t)c;
   };
   int64_t C = std::min<int64_t>(ntiles, (int64_t)(avail / (ao_per_tile + 1)));
   while (C > 0 && chunk_bytes(C) > avail) --C;
@@ -173,7 +173,8 @@ int eval_local_noalloc(ctc_molecule* mol, const double* d_points, int64_t n, con
     const unsigned g = (unsigned)(((int64_t)tb.C * TP + 255) / 256);
     tile_gather_kernel<<<g, 256, 0, st>>>(d_points, perm, n, t0, tb);
     CTC_CUDA_TRY(cudaGetLastError());
-    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, 128, mol->d_stats);
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, 128, mol->d_stats,
+                                                 mol->d_status);
     CTC_CUDA_TRY(cudaGetLastError());
     if ((rc = launch_ao_tiles(mol, tb, plan.deriv, st)) != CTC_OK) return rc;
     if ((rc = fp64_local_tiles(mol, plan, tb, prm, out, st)) != CTC_OK) return rc;

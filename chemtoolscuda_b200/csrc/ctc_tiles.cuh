@@ -10,6 +10,7 @@
 #pragma once
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <functional>
@@ -107,24 +108,17 @@ __global__ void tile_cubic_kernel(PointSrc src, int nx, int TX, int TY, int TZ, 
   tb.out[gid] = v ? (i * src.ny + k) * (int64_t)src.nz + l : -1;
 }
 
-// One CTA per tile: bounding sphere of the tile's points, then the ordered
-// list of segments whose screening sphere meets it.
-__global__ void __launch_bounds__(kTileThreads)
-    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb, int rows,
-                  double* __restrict__ stats) {
-  using Scan = cub::BlockScan<int, kTileThreads>;
-  __shared__ typename Scan::TempStorage scan_tmp;
-  __shared__ int s_sl[kSortCap], s_k0[kSortCap], s_cnt[8];
+// Bounding sphere of one tile's points, computed by a whole block of
+// kTileThreads threads: centre = mean of the finite points (padding repeats a
+// real point; a point with a non-finite coordinate gets NaN outputs and must
+// not move the sphere of its tile mates), radius = largest distance from it,
+// widened by a relative 1e-12 plus 1e-9 bohr; -1e300 when no point is finite.
+// The screening kernel and the capacity pre-pass both use this code, so they
+// see the same sphere to the last bit.
+__device__ void tile_sphere(const double* __restrict__ xyz, int TP, double* sctr, double* srad) {
   __shared__ double red[3][kTileThreads / 32];
-  __shared__ double sctr[3], srad;
-  __shared__ int base_s, base_k;
-  const int t = blockIdx.x, TP = tb.TP;
-  const double* xyz = tb.xyz + (int64_t)t * TP * 3;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // centre = mean of the tile's finite points (padding repeats a real point;
-  // a point with a non-finite coordinate gets NaN outputs and must not move
-  // the sphere of its tile mates)
   __shared__ int s_nfin;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_nfin = 0;
   __syncthreads();
   double c[3] = {0, 0, 0};
@@ -159,10 +153,65 @@ __global__ void __launch_bounds__(kTileThreads)
   if (threadIdx.x == 0) {
     double m = 0;
     for (int w = 0; w < kTileThreads / 32; ++w) m = fmax(m, red[0][w]);
-    // a tile without a finite point keeps no segment (radius -1)
-    srad = s_nfin ? sqrt(m) * (1.0 + 1e-12) + 1e-9 : -1e300;
+    // a tile without a finite point keeps no segment
+    *srad = s_nfin ? sqrt(m) * (1.0 + 1e-12) + 1e-9 : -1e300;
+  }
+  __syncthreads();
+}
+
+// Is segment sg significant on the tile sphere (ctr, rad)?  Every AO value and
+// derivative of the segment is below 1e-18 beyond sqrt(rcut2) of its centre.
+__device__ __forceinline__ bool seg_significant(const DevSeg& sg, const double* ctr, double rad) {
+  const double dx = sg.cx - ctr[0], dy = sg.cy - ctr[1], dz = sg.cz - ctr[2];
+  const double d = sqrt(dx * dx + dy * dy + dz * dz);
+  return d <= sqrt(sg.rcut2) + rad;
+}
+
+// Status code of a tile whose compact AO set exceeds the batch's capacity
+// (cannot happen when the capacity comes from tile_capacity_kernel).
+constexpr int32_t kStatusCapacity = 0x7201;
+
+// Capacity pre-pass: the largest padded compact AO count of a batch of tiles
+// (atomicMax into *kmax).  One block per tile.
+__global__ void __launch_bounds__(kTileThreads)
+    tile_capacity_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb, int* kmax) {
+  __shared__ double sctr[3], srad;
+  __shared__ int part[kTileThreads / 32];
+  const int t = blockIdx.x;
+  tile_sphere(tb.xyz + (int64_t)t * tb.TP * 3, tb.TP, sctr, &srad);
+  int cnt = 0;
+  for (int s = threadIdx.x; s < nseg; s += kTileThreads) {
+    const DevSeg sg = segs[s];
+    if (seg_significant(sg, sctr, srad)) cnt += ncomp_of_type_dev(sg.type);
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int w = 0; w < kTileThreads / 32; ++w) tot += part[w];
+    atomicMax(kmax, (tot + kKtAlign - 1) / kKtAlign * kKtAlign);
+  }
+}
+
+// One CTA per tile: bounding sphere of the tile's points, then the ordered
+// list of segments whose screening sphere meets it.
+__global__ void __launch_bounds__(kTileThreads)
+    screen_kernel(const DevSeg* __restrict__ segs, int nseg, TileBatch tb, int rows,
+                  double* __restrict__ stats, int32_t* __restrict__ status) {
+  using Scan = cub::BlockScan<int, kTileThreads>;
+  __shared__ typename Scan::TempStorage scan_tmp;
+  __shared__ int s_sl[kSortCap], s_k0[kSortCap], s_cnt[8];
+  __shared__ double sctr[3], srad;
+  __shared__ int base_s, base_k;
+  __shared__ int s_over_s, s_over_k;  // first segment beyond the capacity
+  const int t = blockIdx.x, TP = tb.TP;
+  tile_sphere(tb.xyz + (int64_t)t * TP * 3, TP, sctr, &srad);
+  if (threadIdx.x == 0) {
     base_s = 0;
     base_k = 0;
+    s_over_s = INT_MAX;
+    s_over_k = INT_MAX;
   }
   __syncthreads();
   const double rad = srad;
@@ -175,10 +224,7 @@ __global__ void __launch_bounds__(kTileThreads)
     DevSeg sg;
     if (s < nseg) {
       sg = segs[s];
-      const double dx = sg.cx - sctr[0], dy = sg.cy - sctr[1], dz = sg.cz - sctr[2];
-      const double d = sqrt(dx * dx + dy * dy + dz * dz);
-      const double lim = sqrt(sg.rcut2) + rad;
-      if (d <= lim) {
+      if (seg_significant(sg, sctr, rad)) {
         sig = 1;
         nc = ncomp_of_type_dev(sg.type);
       }
@@ -192,7 +238,15 @@ __global__ void __launch_bounds__(kTileThreads)
       const int ks = base_k + pos.y;
       sl[base_s + pos.x] = s;
       k0[base_s + pos.x] = ks;
-      for (int q = 0; q < nc; ++q) am[ks + q] = sg.ao0 + q;
+      if (ks + nc <= tb.Kcap) {
+        for (int q = 0; q < nc; ++q) am[ks + q] = sg.ao0 + q;
+      } else {
+        // never with a capacity from the pre-pass or Kcap = Mpad: the tile is
+        // cut at this segment and the call reports kStatusCapacity
+        atomicMin(&s_over_s, base_s + pos.x);
+        atomicMin(&s_over_k, ks);
+        atomicExch(status, kStatusCapacity);
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -205,7 +259,7 @@ __global__ void __launch_bounds__(kTileThreads)
   // (counting sort; compact positions k0 keep the AO order), so that the
   // warps of a CTA run one type's evaluation code at a time instead of
   // alternating between the types' large unrolled bodies.
-  const int ns = base_s;
+  const int ns = min(base_s, s_over_s);
   if (ns <= kSortCap) {
     if (threadIdx.x < 8) s_cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -232,11 +286,11 @@ __global__ void __launch_bounds__(kTileThreads)
       k0[pos] = s_k0[i];
     }
   }
-  const int kt_true = base_k;
-  const int kt = (kt_true + kKtAlign - 1) / kKtAlign * kKtAlign;
+  const int kt_true = min(base_k, s_over_k);
+  const int kt = min((kt_true + kKtAlign - 1) / kKtAlign * kKtAlign, tb.Kcap);
   for (int k = kt_true + threadIdx.x; k < kt; k += kTileThreads) am[k] = -1;
   if (threadIdx.x == 0) {
-    tb.nsig[t] = base_s;
+    tb.nsig[t] = ns;
     tb.ktrue[t] = kt_true;
     tb.kt[t] = kt;
     int npts = 0;
@@ -516,8 +570,8 @@ struct Carve {
   }
 };
 
-size_t tile_bytes(const ctc_molecule* mol, int C, int TP) {
-  const size_t Kcap = mol->Mpad;
+size_t tile_bytes(const ctc_molecule* mol, int C, int TP, int Kcap_) {
+  const size_t Kcap = Kcap_;
   size_t b = 0;
   auto add = [&](size_t x) { b = (b + 255) / 256 * 256 + x; };
   add(sizeof(double) * C * TP * 3);
@@ -554,43 +608,7 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
   } else {
     ntiles = (n + TP - 1) / TP;
   }
-  // chunk of tiles: AO block (nq x TP x Mpad doubles per tile) within
-  // min(12 GiB, a quarter of the free device memory) (CTC_CHUNK_BYTES
-  // overrides), at least one full wave of CTAs on 148 SMs.  Larger chunks
-  // amortise the per-chunk launches and tails: on the 215^3 benchmark cube
-  // 6 GiB gave 20.95 M points/s, 12 GiB 21.46 M, 24 GiB 21.60 M.
-  const size_t ao_per_tile = sizeof(double) * (size_t)nq * TP * mol->Mpad;
-  size_t budget = (size_t)12 << 30;
-  {
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 4);
-    else cudaGetLastError();  // clear the error; keep the default
-  }
-  if (const char* env = std::getenv("CTC_CHUNK_BYTES")) {
-    const long long v = std::atoll(env);
-    if (v > 0) budget = (size_t)v;
-  }
-  int64_t C = std::max<int64_t>(148, (int64_t)(budget / ao_per_tile));
-  C = std::min<int64_t>(C, ntiles);
   int rc;
-  if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;
-  if ((rc = mol->ws_misc.ensure(tile_bytes(mol, (int)C, TP), st)) != CTC_OK) return rc;
-  TileBatch tb;
-  tb.TP = TP;
-  tb.Kcap = mol->Mpad;
-  tb.nq = nq;
-  tb.ao = (double*)mol->ws_ao.p;
-  {
-    Carve cv{(char*)mol->ws_misc.p};
-    tb.xyz = cv.take<double>((size_t)C * TP * 3);
-    tb.out = cv.take<int64_t>((size_t)C * TP);
-    tb.nsig = cv.take<int32_t>(C);
-    tb.ktrue = cv.take<int32_t>(C);
-    tb.kt = cv.take<int32_t>(C);
-    tb.segs = cv.take<int32_t>((size_t)C * mol->nseg);
-    tb.k0 = cv.take<int32_t>((size_t)C * mol->nseg);
-    tb.aomap = cv.take<int32_t>((size_t)C * tb.Kcap);
-  }
   // explicit points: Morton order over the molecule's box padded by 12 bohr
   int32_t* perm = nullptr;
   if (!src.cubic) {
@@ -627,8 +645,8 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
                                                  kMortonSortBits, st));
     mol->host_launches += 2;
   }
-  for (int64_t t0 = 0; t0 < ntiles; t0 += C) {
-    tb.C = (int)std::min<int64_t>(C, ntiles - t0);
+  // tile points of tiles [t0, t0 + tb.C)
+  auto tile_points = [&](const TileBatch& tb, int64_t t0) -> int {
     const int64_t npts = (int64_t)tb.C * TP;
     const unsigned g = (unsigned)((npts + 255) / 256);
     if (src.cubic)
@@ -636,7 +654,78 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     else
       tile_gather_kernel<<<g, 256, 0, st>>>(src.pts, perm, n, t0, tb);
     CTC_CUDA_TRY(cudaGetLastError());
-    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, rows, mol->d_stats);
+    return CTC_OK;
+  };
+  // chunk of tiles: AO block (nq x TP x Kcap doubles per tile) within
+  // min(12 GiB, a quarter of the free device memory) (CTC_CHUNK_BYTES
+  // overrides), at least one full wave of CTAs on 148 SMs.  Larger chunks
+  // amortise the per-chunk launches and tails: on the 215^3 benchmark cube
+  // 6 GiB gave 20.95 M points/s, 12 GiB 21.46 M, 24 GiB 21.60 M.
+  size_t budget = (size_t)12 << 30;
+  {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 4);
+    else cudaGetLastError();  // clear the error; keep the default
+  }
+  if (const char* env = std::getenv("CTC_CHUNK_BYTES")) {
+    const long long v = std::atoll(env);
+    if (v > 0) budget = (size_t)v;
+  }
+  // Capacity of a tile's compact AO set: Mpad always suffices.  When a chunk
+  // sized for Mpad columns would hold fewer than four waves of tiles (large
+  // bases: the 1 000-atom molecule keeps ~350 of 16 128 functions per tile), a
+  // count-only screening pass over every tile of the call finds the largest
+  // compact set and the workspace is sized for that instead.  It waits for
+  // the stream once (to read the count back); smaller bases skip it.
+  int Kcap = mol->Mpad;
+  if ((int64_t)(budget / (sizeof(double) * (size_t)nq * TP * mol->Mpad)) < 4 * 148 && ntiles > 148) {
+    const int64_t PB = std::min<int64_t>(ntiles, 16384);
+    const size_t pb_bytes = sizeof(double) * (size_t)PB * TP * 3 + sizeof(int64_t) * (size_t)PB * TP + 1024;
+    if ((rc = mol->ws_cap.ensure(pb_bytes, st)) != CTC_OK) return rc;
+    TileBatch pb;
+    pb.TP = TP;
+    Carve cv{(char*)mol->ws_cap.p};
+    int* d_kmax = cv.take<int>(1);
+    pb.xyz = cv.take<double>((size_t)PB * TP * 3);
+    pb.out = cv.take<int64_t>((size_t)PB * TP);
+    CTC_CUDA_TRY(cudaMemsetAsync(d_kmax, 0, sizeof(int), st));
+    for (int64_t t0 = 0; t0 < ntiles; t0 += PB) {
+      pb.C = (int)std::min<int64_t>(PB, ntiles - t0);
+      if ((rc = tile_points(pb, t0)) != CTC_OK) return rc;
+      tile_capacity_kernel<<<pb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, pb, d_kmax);
+      CTC_CUDA_TRY(cudaGetLastError());
+      mol->host_launches += 2;
+    }
+    CTC_CUDA_TRY(cudaMemcpyAsync(mol->h_status + 1, d_kmax, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CTC_CUDA_TRY(cudaStreamSynchronize(st));
+    Kcap = std::min(mol->Mpad, std::max(kKtAlign, (int)mol->h_status[1]));
+  }
+  const size_t ao_per_tile = sizeof(double) * (size_t)nq * TP * Kcap;
+  int64_t C = std::max<int64_t>(148, (int64_t)(budget / ao_per_tile));
+  C = std::min<int64_t>(C, ntiles);
+  if ((rc = mol->ws_ao.ensure(ao_per_tile * C, st)) != CTC_OK) return rc;
+  if ((rc = mol->ws_misc.ensure(tile_bytes(mol, (int)C, TP, Kcap), st)) != CTC_OK) return rc;
+  TileBatch tb;
+  tb.TP = TP;
+  tb.Kcap = Kcap;
+  tb.nq = nq;
+  tb.ao = (double*)mol->ws_ao.p;
+  {
+    Carve cv{(char*)mol->ws_misc.p};
+    tb.xyz = cv.take<double>((size_t)C * TP * 3);
+    tb.out = cv.take<int64_t>((size_t)C * TP);
+    tb.nsig = cv.take<int32_t>(C);
+    tb.ktrue = cv.take<int32_t>(C);
+    tb.kt = cv.take<int32_t>(C);
+    tb.segs = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.k0 = cv.take<int32_t>((size_t)C * mol->nseg);
+    tb.aomap = cv.take<int32_t>((size_t)C * tb.Kcap);
+  }
+  for (int64_t t0 = 0; t0 < ntiles; t0 += C) {
+    tb.C = (int)std::min<int64_t>(C, ntiles - t0);
+    if ((rc = tile_points(tb, t0)) != CTC_OK) return rc;
+    screen_kernel<<<tb.C, kTileThreads, 0, st>>>(mol->d_segs, mol->nseg, tb, rows, mol->d_stats,
+                                                 mol->d_status);
     CTC_CUDA_TRY(cudaGetLastError());
     {
       ProfScope ps(mol, 1, st);

@@ -282,6 +282,34 @@ def surface_points(mol: SyntheticMolecule, seed: int = 0, scales=(1.4, 1.6, 1.8,
     return pts
 
 
+def submolecule(mol: SyntheticMolecule, natom: int, nocc: int, seed: int = 0) -> SyntheticMolecule:
+    """The first ``natom`` atoms of ``mol`` with their shells and a fresh density
+    matrix D = 2 C C^T of ``nocc`` occupied columns (seeded)."""
+    shells = [sh for sh in mol.shells if sh.atom < natom]
+    M = sum(nfunc(a) for sh in shells for a in sh.angmoms)
+    D = make_density_matrix(np.random.default_rng(seed), M, nocc)
+    return SyntheticMolecule(coords=mol.coords[:natom].copy(), numbers=mol.numbers[:natom].copy(),
+                             charges=mol.charges[:natom].copy(), shells=shells, D=D,
+                             name=f"{mol.name}[:{natom}]", meta=dict(mol.meta, natom=natom, nocc=nocc))
+
+
+def reference_esp_fit(mol: SyntheticMolecule, limit_bytes: int = 60000) -> int:
+    """Largest number of leading atoms whose basis fits the reference's ESP: its
+    segmented basis -- per segment x, y, z, K, l and K exponents and K
+    coefficients, plus one header double -- must stay below 60 000 bytes of
+    constant memory (src/basis_to_gpu.cu:60-120, src/evaluate_electrostatic.cu:10166-10176)."""
+    per_atom = np.zeros(len(mol.coords))
+    for sh in mol.shells:
+        per_atom[sh.atom] += len(sh.angmoms) * (5 + 2 * len(sh.exponents))
+    used, k = 1.0, 0
+    for a in range(len(mol.coords)):
+        if 8 * (used + per_atom[a]) >= limit_bytes:
+            break
+        used += per_atom[a]
+        k = a + 1
+    return k
+
+
 # The ESP workload asks for 1e6 points on the four nested surfaces of the
 # 100-atom molecule; at 20 points per bohr^2 those surfaces hold ~277 000
 # points, so the workload samples them at the density that gives ~1e6.
