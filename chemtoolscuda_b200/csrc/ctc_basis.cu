@@ -41,6 +41,28 @@ std::mutex g_sm_mu;
 std::vector<std::pair<int, int>> g_sm_count;  // (device, SM count)
 }  // namespace
 
+// d_D (Mpad x Mpad, internal AO order, zero padded) from a caller's D
+// (M x M, caller's order): d_D[i][j] = D[perm[i]][perm[j]].
+__global__ void permute_density_kernel(const double* __restrict__ D, int M, int Mpad,
+                                       const int32_t* __restrict__ perm, double* __restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)Mpad * Mpad) return;
+  const int i = (int)(e / Mpad), j = (int)(e % Mpad);
+  out[e] = (i < M && j < M) ? D[(int64_t)perm[i] * M + perm[j]] : 0.0;
+}
+
+int refresh_host_density(ctc_molecule* m) {
+  if (!m->host_D_stale) return CTC_OK;
+  const int M = m->M, Mp = m->Mpad;
+  std::vector<double> pad((size_t)Mp * Mp);
+  CTC_CUDA_TRY(cudaDeviceSynchronize());
+  CTC_CUDA_TRY(cudaMemcpy(pad.data(), m->d_D, sizeof(double) * pad.size(), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < M; ++i)
+    std::memcpy(&m->D[(size_t)i * M], &pad[(size_t)i * Mp], sizeof(double) * M);
+  m->host_D_stale = false;
+  return CTC_OK;
+}
+
 int ensure_smem_attr(const void* kernel, int bytes) {
   int dev = 0;
   CTC_CUDA_TRY(cudaGetDevice(&dev));
@@ -410,6 +432,7 @@ int ctc_molecule_create(const ctc_basis* b, int32_t natom, const double* atom_xy
   ALLOC_COPY(m->d_ao_atom, m->ao_atom.data(), m->ao_atom.size());
   ALLOC_COPY(m->d_D, Dpad.data(), MM);
   ALLOC_COPY(m->d_ao_iperm, iperm.data(), iperm.size());
+  ALLOC_COPY(m->d_ao_perm, m->ao_perm.data(), m->ao_perm.size());
 #undef ALLOC_COPY
   if (cudaMalloc((void**)&m->d_status, sizeof(int32_t)) != cudaSuccess ||
       cudaMemset(m->d_status, 0, sizeof(int32_t)) != cudaSuccess ||
@@ -436,6 +459,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   cudaFree(m->d_ao_atom);
   cudaFree(m->d_D);
   cudaFree(m->d_ao_iperm);
+  cudaFree(m->d_ao_perm);
   cudaFree(m->d_Dsl);
   cudaFree(m->d_Dscale);
   cudaFree(m->d_status);
@@ -462,20 +486,12 @@ int ctc_molecule_set_density_matrix(ctc_molecule* m, const double* d_D, void* st
   if (!m || !d_D) return fail(CTC_ERR_INVALID, "set_density_matrix: null argument");
   cudaStream_t st = (cudaStream_t)stream;
   const int M = m->M, Mp = m->Mpad;
-  std::vector<double> h((size_t)M * M);
-  CTC_CUDA_TRY(cudaMemcpyAsync(h.data(), d_D, sizeof(double) * M * M, cudaMemcpyDeviceToHost, st));
-  CTC_CUDA_TRY(cudaStreamSynchronize(st));
-  std::vector<double> pad((size_t)Mp * Mp, 0.0);
-  for (int i = 0; i < M; ++i) {
-    const double* src = &h[(size_t)m->ao_perm[i] * M];
-    for (int j = 0; j < M; ++j) {
-      const double v = src[m->ao_perm[j]];
-      m->D[(size_t)i * M + j] = v;
-      pad[(size_t)i * Mp + j] = v;
-    }
-  }
-  CTC_CUDA_TRY(cudaMemcpyAsync(m->d_D, pad.data(), sizeof(double) * pad.size(), cudaMemcpyHostToDevice, st));
-  CTC_CUDA_TRY(cudaStreamSynchronize(st));
+  const int64_t total = (int64_t)Mp * Mp;
+  ctc::permute_density_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(d_D, M, Mp, m->d_ao_perm,
+                                                                               m->d_D);
+  CTC_CUDA_TRY(cudaGetLastError());
+  // the host copy (used only to build the ESP tables) is fetched again when needed
+  m->host_D_stale = true;
   m->dsl_valid = false;
   m->esp_valid = false;
   return CTC_OK;

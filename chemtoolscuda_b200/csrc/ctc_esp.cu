@@ -298,6 +298,7 @@ void destroy_esp(ctc_molecule* mol) {
 
 static int build_esp(ctc_molecule* mol) {
   destroy_esp(mol);
+  if (int rc = refresh_host_density(mol); rc != CTC_OK) return rc;
   for (const DevSeg& s : mol->segs)
     if (s.l > 4) return fail(CTC_ERR_UNSUPPORTED, "ESP: angular momentum above g");
   const int nseg = mol->nseg, M = mol->M;

@@ -20,6 +20,8 @@ int fail(int code, const std::string& msg);
 int ensure_smem_attr(const void* kernel, int bytes);
 // Streaming multiprocessors of the current device (cached per device).
 int device_sm_count(int* out);
+__global__ void permute_density_kernel(const double* __restrict__ D, int M, int Mpad,
+                                       const int32_t* __restrict__ perm, double* __restrict__ out);
 
 #define CTC_CUDA_TRY(expr)                                                               \
   do {                                                                                   \
@@ -144,6 +146,8 @@ struct ctc_molecule {
   std::vector<int32_t> ao_atom;              // AO -> atom (internal order)
   std::vector<int32_t> ao_perm;              // internal AO -> caller's AO
   int32_t* d_ao_iperm = nullptr;             // caller's AO -> internal AO
+  int32_t* d_ao_perm = nullptr;              // internal AO -> caller's AO
+  bool host_D_stale = false;                 // D replaced on the device since the host copy was made
   // device tables
   ctc::DevSeg* d_segs = nullptr;
   double* d_alpha = nullptr;
@@ -221,6 +225,10 @@ int fp64_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& 
 
 // per-point finalisation shared by the contraction kernels (ctc_local.cu)
 struct LocalSums;
+
+// Host copy of D (internal order) brought up to date after a device-side
+// replacement (ctc_molecule_set_density_matrix); synchronises the device.
+int refresh_host_density(ctc_molecule* mol);
 
 // ---- ESP (ctc_esp.cu) ----
 int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out, cudaStream_t st);

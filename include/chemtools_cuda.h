@@ -105,8 +105,10 @@ int ctc_molecule_destroy(ctc_molecule* mol);
 int ctc_molecule_nbasis(const ctc_molecule* mol);
 int ctc_molecule_natom(const ctc_molecule* mol);
 
-/* Replace D from device memory (stream-ordered).  Replaces the per-call
- * cublasSetMatrix uploads (e.g. src/evaluate_density.cu:777). */
+/* Replace D from device memory (nbasis x nbasis, row-major, symmetric):
+ * stream-ordered, a permuting copy on the device with no host round trip.
+ * Replaces the per-call cublasSetMatrix uploads (e.g.
+ * src/evaluate_density.cu:777). */
 int ctc_molecule_set_density_matrix(ctc_molecule* mol, const double* d_D, void* stream);
 
 /* Move the atoms (host (natom,3)); the shells move with their atoms. */

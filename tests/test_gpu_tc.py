@@ -150,3 +150,33 @@ def test_tc_headline_configuration_full_size():
     pts = S.cube_points(origin, axes, shape)[idx]
     ref, sc = _oracle(mol, pts, KEYS)
     _compare("c2 headline 215^3", got, ref, sc, KEYS)
+
+
+@pytest.mark.parametrize("precision", [ctc_abi.PREC_FP64, ctc_abi.PREC_TC], ids=["fp64", "tc"])
+def test_capacity_prepass_matches_default_workspace(torch_cuda, precision):
+    """A small chunk budget (CTC_CHUNK_BYTES) makes the pipeline size its tile
+    workspaces by a count-only screening pass (the largest compact AO set of
+    the call) instead of the whole basis; results must not change, on random
+    points (Morton tiles) and on a cubic grid."""
+    mol = S.make_molecule("c2", seed=4, natom=40, box=12.0, nocc=80)
+    rng = np.random.default_rng(8)
+    pts = S.random_points(rng, mol, 12000, pad=2.0)
+    origin, axes = S.cube_grid(mol, 0.3, (24, 26, 28))
+    keys = ("rho", "grad", "hess", "lap", "tau_pd")
+    m = ctc_abi.Mol(mol.flat(), mol.coords, mol.charges, mol.D)
+    base = m.eval_local(pts, keys, precision)
+    cbase = m.eval_cubic(origin, axes, (24, 26, 28), keys=keys, precision=precision)
+    os.environ["CTC_CHUNK_BYTES"] = str(8 << 20)
+    try:
+        small = m.eval_local(pts, keys, precision)
+        csmall = m.eval_cubic(origin, axes, (24, 26, 28), keys=keys, precision=precision)
+    finally:
+        del os.environ["CTC_CHUNK_BYTES"]
+    assert m.sync_status() == 0
+    for k in keys:
+        np.testing.assert_allclose(small[k], base[k], rtol=1e-13, atol=1e-16, err_msg=k)
+        np.testing.assert_allclose(csmall[k], cbase[k], rtol=1e-13, atol=1e-16, err_msg=k)
+    ref, sc = _oracle(mol, pts[:300], keys)
+    _compare("prepass", {k: v[:300] for k, v in small.items()}, ref, sc, keys,
+             1e-10 if precision == ctc_abi.PREC_FP64 else TC_RTOL)
+    m.close()
