@@ -389,21 +389,31 @@ static int build_esp(ctc_molecule* mol) {
   std::vector<std::thread> th;
   for (unsigned t = 0; t < nthr; ++t) th.emplace_back(worker, t);
   for (auto& t : th) t.join();
-  // drop the weakest pairs while their summed bound stays within the budget
+  // drop the weakest pairs while their summed bound stays within the budget:
+  // pairs are ranked by (bound, thread, position) and exactly the accumulated
+  // prefix is dropped, so ties at the cut never drop more than the budget
   {
-    std::vector<double> bounds;
-    for (auto& o : outs)
-      for (auto& po : o) bounds.push_back(po.bound);
-    std::sort(bounds.begin(), bounds.end());
-    double acc = 0.0, cut = 0.0;
-    for (double b : bounds) {
-      if (acc + b > budget) break;
-      acc += b;
-      cut = b;
+    struct Ranked { double bound; uint32_t list, pos; };
+    std::vector<Ranked> rk;
+    for (uint32_t l = 0; l < outs.size(); ++l)
+      for (uint32_t i = 0; i < outs[l].size(); ++i) rk.push_back({outs[l][i].bound, l, i});
+    std::sort(rk.begin(), rk.end(), [](const Ranked& a, const Ranked& b) {
+      return a.bound != b.bound ? a.bound < b.bound : (a.list != b.list ? a.list < b.list : a.pos < b.pos);
+    });
+    std::vector<std::vector<char>> drop(outs.size());
+    for (size_t l = 0; l < outs.size(); ++l) drop[l].assign(outs[l].size(), 0);
+    double acc = 0.0;
+    for (const Ranked& r : rk) {
+      if (acc + r.bound > budget) break;
+      acc += r.bound;
+      drop[r.list][r.pos] = 1;
     }
-    for (auto& o : outs)
-      o.erase(std::remove_if(o.begin(), o.end(), [&](const PairOut& po) { return po.bound <= cut; }),
-              o.end());
+    for (size_t l = 0; l < outs.size(); ++l) {
+      size_t w = 0;
+      for (size_t i = 0; i < outs[l].size(); ++i)
+        if (!drop[l][i]) outs[l][w++] = std::move(outs[l][i]);
+      outs[l].resize(w);
+    }
   }
   // gather, sorted by L, into batches of equal L
   std::vector<EspPair> pairs;

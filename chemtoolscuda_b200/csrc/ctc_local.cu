@@ -69,9 +69,8 @@ int eval_local(ctc_molecule* mol, const PointSrc& src, int64_t n, int precision,
     if (int rc = prepare_tc(mol, st); rc != CTC_OK) return rc;
   }
   // points per tile: 128 rows of the contraction (32 points x 4 quantities or
-  // 128 points x phi); the tensor-core path pairs two 128-row blocks on one
-  // B operand, so its tiles of phi and grad phi rows hold 64 points
-  const int TP = (precision == CTC_PREC_TC_SPLIT && plan.nqa == 4) ? 64 : 128 / plan.nqa;
+  // 128 points x phi)
+  const int TP = 128 / plan.nqa;
   const int rows = TP * plan.nqa;
   // tensor-core path: the AO kernel also writes the int8 digit planes
   const std::function<int(const TileBatch&)> sliced_ao = [&](const TileBatch& tb) {

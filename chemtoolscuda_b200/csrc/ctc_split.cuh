@@ -5,21 +5,25 @@
 // (|x| < 2^e), and rounded to a fixed-point integer written in balanced
 // base-256 digits (|d| <= 128), one int8 plane per digit, most significant
 // first:
-//   * D rows (B operand): I = rint(x 2^(30-e)), |I| <= 2^30, four digits;
+//   * D rows (B operand): I = rint(x 2^(38-e)), |I| <= 2^38, five digits;
 //   * tile rows of phi and grad phi (A operand): I = rint(x 2^(38-e)),
 //     |I| <= 2^38, five digits.
-// The A rows get the extra digit because a row's error is set by its largest
-// entry: an AO row with one steep function (a tight g shell near its centre)
-// and many small ones loses relative precision on the small ones, which
-// showed as errors of 2e-8 of the sum of absolute terms with 31 bits; D rows
-// do not have this spread.
+// 31 bits (four digits) are not enough on either side.  An AO row's error is
+// set by its largest entry: a row with one steep function (a tight g shell
+// near its centre) and many small ones loses relative precision on the
+// small ones (2e-8 of the sum of absolute terms with 31 bits).  A D row
+// whose largest entry is a core element loses the small valence entries of
+// the same row: near nuclei the Hessian and gradient reached 1.8e-8 (Kr and
+// C atoms of the reference's fixtures) and 2.8e-8 (the 200-atom benchmark
+// molecule, 0.004 bohr from a nucleus) with 31-bit D rows, 1e-9 and 2.5e-9
+// with 39 bits (CPU emulation of this split).
 #pragma once
 
 #include <cstdint>
 
 namespace ctc {
 
-constexpr int kSplitPlanesD = 4;  // digit planes of D (B operand)
+constexpr int kSplitPlanesD = 5;  // digit planes of D (B operand)
 constexpr int kSplitPlanesA = 5;  // digit planes of the tile rows (A operand)
 constexpr int kSplitRows = 128;   // rows of one block of a tile operand (MMA M)
 
@@ -29,7 +33,7 @@ constexpr int kSplitRows = 128;   // rows of one block of a tile operand (MMA M)
 // With nqa = 4 point p's quantity q is row (p / 32) * 128 + q * 32 + p % 32,
 // so every block holds 32 points x 4 quantities; with nqa = 1 row = point.
 __host__ __device__ constexpr int split_tile_rows(int TP, int nqa) { return TP * nqa; }
-constexpr int kFixedBitsD = 30;   // |I| <= 2^30
+constexpr int kFixedBitsD = 38;   // |I| <= 2^38
 constexpr int kFixedBitsA = 38;   // |I| <= 2^38
 
 // Lowest row exponent used: rows whose largest |x| is below 2^-980 are
@@ -46,6 +50,14 @@ constexpr int kMinScaleExponent = -980;
 __device__ __forceinline__ uint32_t pack_digits(int32_t I) {
   const uint32_t u = (uint32_t)(I + 0x808080) ^ 0x808080u;
   return __byte_perm(u, 0u, 0x0123);
+}
+
+// The five balanced digits of |I| <= 2^38 in one 64-bit word: bytes 0-3 the
+// four most significant (pack_digits of the upper part), byte 4 the lowest
+// digit d4 (balanced, as int8); bytes 5-7 zero.
+__device__ __forceinline__ uint64_t pack_digits5(long long I) {
+  const int32_t d4 = (int32_t)(((I + 128) & 255) - 128);
+  return (uint64_t)pack_digits((int32_t)((I - d4) >> 8)) | ((uint64_t)(uint32_t)(d4 & 255) << 32);
 }
 
 // rint(y) for |y| < 2^31 (round half to even) with one FP64 add: the sum

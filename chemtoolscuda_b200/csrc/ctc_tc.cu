@@ -9,21 +9,21 @@
 //   * every A row r is scaled by 2^-e_r (e_r from the row's largest |value|)
 //     and rounded to I_A = rint(x 2^(38 - e_r)), five balanced base-256 digits
 //     a_0..a_4 (|a_i| <= 128, I_A = sum_i a_i 256^(4-i)); every D row nu by
-//     2^-f_nu, I_D = rint(y 2^(30 - f_nu)), four digits b_0..b_3; one int8
+//     2^-f_nu, I_D = rint(y 2^(38 - f_nu)), five digits b_0..b_4; one int8
 //     plane per digit;
-//   * the 14 digit products with i + j <= 4 are accumulated on INT8 tensor
+//   * the 15 digit products with i + j <= 4 are accumulated on INT8 tensor
 //     cores (tcgen05.mma kind::i8, int32 accumulators in TMEM), one TMEM
 //     accumulator per level L = i + j;  int32 accumulation is exact as long
 //     as the compact K of a tile stays below 16 384;
-//   * the epilogue forms G = 2^(e_r + f_nu - 68) sum_L acc_L 2^(56 - 8 L) in
+//   * the epilogue forms G = 2^(e_r + f_nu - 76) sum_L acc_L 2^(64 - 8 L) in
 //     FP64 and reduces it against the FP64 AO values (same epilogue sums as
 //     the FP64 path).
-// The dropped products (i + j >= 5) are below 2^-36 of the row/column scale.
+// The dropped products (i + j >= 5) are below 2^-40 of the row/column scale.
 //
 // Kernel roles (288 threads, one persistent CTA per SM taking the chunk's
 // tiles largest first from a launch-wide counter): warps 0-3 produce the
 // operands of each K block (one thread issues the TMA loads of the five A
-// planes; all 128 threads gather the four D planes by compact index from the
+// planes; all 128 threads gather the five D planes by compact index from the
 // packed copy of D and write them in the 64-byte-swizzled K-major layout),
 // warp 4 issues the MMAs from one thread and commits them to mbarriers, warps
 // 5-8 drain the TMEM accumulators (one 32-lane quarter each) into an FP64 copy
@@ -144,9 +144,9 @@ __device__ __forceinline__ void tma_load_2d_hint(void* dst, const CUtensorMap* m
       : "memory");
 }
 
-__device__ __forceinline__ uint32_t ldg_u32_hint(const uint32_t* p, uint64_t policy) {
-  uint32_t v;
-  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;\n" : "=r"(v) : "l"(p), "l"(policy));
+__device__ __forceinline__ uint64_t ldg_u64_hint(const uint64_t* p, uint64_t policy) {
+  uint64_t v;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;\n" : "=l"(v) : "l"(p), "l"(policy));
   return v;
 }
 
@@ -174,26 +174,6 @@ __device__ __forceinline__ uint32_t sw64_offset(int row, int k) {
   const int r8 = row & 7;
   const int chunk = (k >> 4) ^ ((r8 >> 1) & 3);
   return (uint32_t)((row >> 3) * 512 + r8 * 64 + chunk * 16 + (k & 15));
-}
-
-// K-major, 32-byte swizzle: 8-row atoms of 256 B, rows 32 B apart (one int8
-// MMA K step per row).
-__device__ __forceinline__ uint64_t umma_desc_sw32(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3fff);        // start address
-  d |= (uint64_t)1 << 16;                         // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(256 >> 4) << 32;                // stride byte offset: 8 rows x 32 B
-  d |= (uint64_t)1 << 46;                         // descriptor version (sm_100)
-  d |= (uint64_t)6 << 61;                         // layout: SWIZZLE_32B
-  return d;
-}
-
-// byte offset of (row, k) inside a K-major SW32 plane (k < 32): the 16-byte
-// half of the row is flipped by bit 2 of the row
-__device__ __forceinline__ uint32_t sw32_offset(int row, int k) {
-  const int r8 = row & 7;
-  const int chunk = (k >> 4) ^ ((r8 >> 2) & 1);
-  return (uint32_t)((row >> 3) * 256 + r8 * 32 + chunk * 16 + (k & 15));
 }
 
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
@@ -367,8 +347,9 @@ __device__ __forceinline__ void store_role(double (*s_sums)[16], int lane, const
 }
 
 // ------------------------------------------------------------------ preparation kernels
-// D (Mpad x Mpad, symmetric) -> packed digit words per element, exponent per row.
-__global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint32_t* __restrict__ Dp,
+// D (Mpad x Mpad, symmetric) -> one 64-bit word of five digits per element
+// (pack_digits5), exponent per row.
+__global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint64_t* __restrict__ Dp,
                                int32_t* __restrict__ fexp) {
   const int row = blockIdx.x;
   const double* d = D + (int64_t)row * Mpad;
@@ -388,14 +369,14 @@ __global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint32_t*
   if (threadIdx.x == 0) fexp[row] = e;
   const double f = split_row_factor(e, kFixedBitsD);
   for (int k = threadIdx.x; k < Mpad; k += blockDim.x)
-    Dp[(int64_t)row * Mpad + k] = pack_digits(rint_i32(d[k] * f));
+    Dp[(int64_t)row * Mpad + k] = pack_digits5(rint_i64(d[k] * f));
 }
 
 // ------------------------------------------------------------------ main kernel
 struct TcArgs {
   TileBatch tb;
   int nqa;
-  const uint32_t* Dp;    // packed D digits, Mpad x Mpad
+  const uint64_t* Dp;    // packed D digits (pack_digits5), Mpad x Mpad
   const int32_t* fexp;   // D row exponents
   const int32_t* eexp;   // A row exponents [C][128]
   int Mpad;
@@ -543,17 +524,17 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 #pragma unroll
         for (int q = 0; q < 4; ++q) mu[q] = am[kb * kBK + k4 + q];
       };
-      auto gather = [&](const int (&nu)[8], const int (&mu)[4], uint32_t (&w)[8][4]) {
+      auto gather = [&](const int (&nu)[8], const int (&mu)[4], uint64_t (&w)[8][4]) {
 #pragma unroll
         for (int q = 0; q < 8; ++q)
 #pragma unroll
           for (int m = 0; m < 4; ++m)
             w[q][m] = (nu[q] >= 0 && mu[m] >= 0)
-                          ? ldg_u32_hint(args.Dp + (int64_t)nu[q] * args.Mpad + mu[m], keep)
-                          : 0u;
+                          ? ldg_u64_hint(args.Dp + (int64_t)nu[q] * args.Mpad + mu[m], keep)
+                          : 0ull;
       };
       int nu[8], mu[4];
-      uint32_t w[8][4];
+      uint64_t w[8][4];
       if (nst > 0) {
         load_idx(0, nu, mu);
         gather(nu, mu, w);
@@ -580,12 +561,19 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         uint8_t* b = sB + s * kBStageBytes;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          // 4 words of 4 digit bytes -> 4 plane words of 4 consecutive mu
+          // 4 words of 5 digit bytes -> 5 plane words of 4 consecutive mu:
+          // digits 0-3 by a byte transpose of the low halves, digit 4 from
+          // byte 4 of each word
           uint32_t pl[4];
-          transpose_bytes4x4(w[q][0], w[q][1], w[q][2], w[q][3], pl);
+          transpose_bytes4x4((uint32_t)w[q][0], (uint32_t)w[q][1], (uint32_t)w[q][2],
+                             (uint32_t)w[q][3], pl);
+          const uint32_t lo = __byte_perm(__byte_perm((uint32_t)(w[q][0] >> 32), (uint32_t)(w[q][1] >> 32), 0x0040),
+                                          __byte_perm((uint32_t)(w[q][2] >> 32), (uint32_t)(w[q][3] >> 32), 0x0040),
+                                          0x5410);
           const uint32_t off = sw64_offset(nrow0 + 8 * q, k4);
 #pragma unroll
-          for (int p = 0; p < kPlanes; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
+          for (int p = 0; p < 4; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
+          *(uint32_t*)(b + 4 * kBPlaneBytes + off) = lo;
         }
         fence_proxy_async();
         mbar_arrive(&full_bar[s]);
@@ -609,14 +597,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     }
   } else if (warp == 4) {
     // ---------------- MMA issuer
-    // One MMA per A digit plane pa and K step: B is the stage's four D planes
+    // One MMA per A digit plane pa and K step: B is the stage's first D planes
     // read as one operand of 64 * nb rows (the planes are contiguous), so the
     // MMA's column block j is the product a_pa b_j and lands at TMEM column
     // (pa + j) * 64, the accumulator of level L = pa + j.  nb = min(4, 5 - pa)
     // keeps L <= 4.  At the first K step of a nu tile pa = 0 (levels 0-3) and
     // pa = 4 (level 4) initialise the 320 columns; every later MMA
-    // accumulates.  Five MMAs of N = 256, 256, 192, 128, 64 replace the 14
-    // N = 64 products: the same work in fewer, wider instructions.
+    // accumulates.  Five MMAs of N = 256, 256, 192, 128, 64 plus a_0 b_4
+    // (N = 64, level 4) replace the 15 N = 64 products: the same work in
+    // fewer, wider instructions.
     const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRows >> 4) << 24);
     int it = 0, gnt = 0;  // stage and nu-tile counters across tiles
     for (int i = 0;; ++i) {
@@ -659,11 +648,15 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 #pragma unroll
               for (int o = 0; o < kPlanesA; ++o) {
                 const int pa = o == 0 ? 0 : (o == 1 ? kPlanesA - 1 : o - 1);  // 0, 4, 1, 2, 3
-                const int nb = kPlanes < kLevels - pa ? kPlanes : kLevels - pa;
+                const int nb = 4 < kLevels - pa ? 4 : kLevels - pa;  // at most N = 256
                 const uint32_t idesc = idesc0 | ((uint32_t)(nb * kN >> 3) << 17);
                 const uint64_t ad = umma_desc_sw64(a0 + pa * kAPlaneBytes + ks * 32);
                 umma_i8(tmem + pa * kN, ad, bd, idesc, (first && o < 2) ? 0u : 1u);
               }
+              // a_0 b_4 (level 4), after level 4 was initialised above
+              umma_i8(tmem + 4 * kN, umma_desc_sw64(a0 + ks * 32),
+                      umma_desc_sw64(b0 + 4 * kBPlaneBytes + ks * 32),
+                      idesc0 | ((uint32_t)(kN >> 3) << 17), 1u);
             }
             umma_commit(&empty_bar[s]);
           }
@@ -712,8 +705,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       const int nnt = (kt + kN - 1) / kN;
       const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
       const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + pc;  // element (q, k) at aop[q*ldq + k*PTS]
-      // G = 2^(e_r + f_nu - 68) sum_L acc_L 2^(56 - 8 L); the drain below forms
-      // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^24
+      // G = 2^(e_r + f_nu - 76) sum_L acc_L 2^(64 - 8 L); the drain below forms
+      // sum_L acc_L 2^(32 - 8 L), so the row factor carries the remaining 2^-44
       const double rowscale = ldexp(1.0, args.eexp[(int64_t)t * kRows + r] - 44);
       double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
       for (int nt = 0; nt < nnt; ++nt, ++gnt) {
@@ -832,433 +825,6 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   }
 }
 
-// ------------------------------------------------------------------ 64-point tiles
-// Tiles of 64 points x {phi, d_x phi, d_y phi, d_z phi}: 256 rows in two
-// 128-row blocks (32 points x 4 quantities each, ctc_split.cuh) that share
-// every B stage.  Each gathered element of D then serves 256 rows instead of
-// 128, halving the producers' gathers per point -- the limit of the
-// 128-row kernel above on large tiles (~2.8 K cycles of gathers against
-// ~1 K of MMA per 64 x 64 stage).  TMEM holds 2 blocks x 5 levels x 48
-// columns (480 of 512), so a nu tile is 48 columns; shared memory holds two
-// stages of 32 K bytes (both blocks' five A planes by TMA, the four D planes
-// gathered, 32-byte swizzle) and the FP64 copy of G (48 x 256).
-namespace pair {
-constexpr int kN = 48;                                  // nu columns per nu tile
-constexpr int kBK = 32;                                 // K bytes per stage (one MMA K step)
-constexpr int kBlocks = 2;                              // 128-row blocks per tile
-constexpr int kStages = 2;
-constexpr int kPts = 64;                                // points per tile
-constexpr int kTileRows = kBlocks * kRows;              // 256
-constexpr int kAPlaneBytes = kRows * kBK;               // 4 KB
-constexpr int kABlockBytes = kPlanesA * kAPlaneBytes;   // 20 KB
-constexpr int kAStageBytes = kBlocks * kABlockBytes;    // 40 KB
-constexpr int kBPlaneBytes = kN * kBK;                  // 1.5 KB
-constexpr int kBStageBytes = kPlanes * kBPlaneBytes;    // 6 KB
-constexpr int kGBytes = kN * kTileRows * 8;             // 96 KB
-constexpr int kSmem = kStages * (kAStageBytes + kBStageBytes) + kGBytes + 1024;
-static_assert(kBlocks * kLevels * kN <= 512, "TMEM columns");
-}  // namespace pair
-// register buffers of the pair kernel's epilogue loads (groups of kEpiGroup
-// columns): fewer than tc_tile_kernel's 8, since the accumulators of both
-// blocks stay live
-#ifndef CTC_PAIR_EPI_BUFFERS
-#define CTC_PAIR_EPI_BUFFERS 6
-#endif
-constexpr int kPairEpiBuffers = CTC_PAIR_EPI_BUFFERS;
-namespace pair {
-static_assert(kAStageBytes % 1024 == 0 && kBStageBytes % 1024 == 0, "stage alignment");
-}  // namespace pair
-
-__global__ void __launch_bounds__(kThreadsTc, 1)
-    tc_pair_kernel(const __grid_constant__ CUtensorMap amap, TcArgs args) {
-  // this kernel's geometry (shadows the 128-row kernel's constants)
-  constexpr int kN = pair::kN, kBK = pair::kBK, kBlocks = pair::kBlocks, kStages = pair::kStages;
-  constexpr int kPts = pair::kPts, kTileRows = pair::kTileRows;
-  constexpr int kAPlaneBytes = pair::kAPlaneBytes, kABlockBytes = pair::kABlockBytes;
-  constexpr int kAStageBytes = pair::kAStageBytes, kBPlaneBytes = pair::kBPlaneBytes;
-  constexpr int kBStageBytes = pair::kBStageBytes;
-  extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kStages], tma_bar[kStages], empty_bar[kStages];
-  __shared__ __align__(8) uint64_t tfull_bar, tempty_bar, done_bar;
-  __shared__ __align__(8) uint64_t tile_full_bar[2], tile_empty_bar[2];
-  __shared__ uint32_t tmem_base_sh;
-  __shared__ int s_abort;
-  __shared__ int s_tile[2];
-  __shared__ int s_epi_tile;
-  __shared__ int s_epi_abort[2];
-  __shared__ double s_sums[kPts][16];
-  __shared__ double s_cscale[2][kN];
-
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* sA = smem;
-  uint8_t* sB = smem + kStages * kAStageBytes;
-  double* sG = (double*)(smem + kStages * (kAStageBytes + kBStageBytes));  // [kN][kTileRows]
-
-  const TileBatch& tb = args.tb;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full_bar[s], 128);
-      mbar_init(&tma_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
-    mbar_init(&tfull_bar, 1);
-    mbar_init(&tempty_bar, 128);
-    mbar_init(&done_bar, 1);
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(&tile_full_bar[i], 1);
-      mbar_init(&tile_empty_bar[i], kTileReaders);
-    }
-    s_abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (warp == 4) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(
-                     smem_u32(&tmem_base_sh)));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
-  }
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = tmem_base_sh;
-  const long long t_start = clock64();
-  long long tr0 = 0, tr1 = 0, tr2 = 0;
-
-  // tile ring and warp-uniform abort decisions as in tc_tile_kernel
-  auto read_tile = [&](int i) -> int {
-    const int slot = i & 1;
-    int t = -1;
-    if (!mbar_wait(&tile_full_bar[slot], (i >> 1) & 1, args.wait_cycles)) {
-      s_abort = 1;
-    } else {
-      t = s_tile[slot];
-    }
-    return t;
-  };
-  auto read_tile_warp = [&](int i) -> int {
-    int t = -1;
-    if (lane == 0) t = read_tile(i);
-    return __shfl_sync(0xffffffffu, t, 0);
-  };
-  auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, s_abort != 0); };
-
-  if (warp < 4) {
-    // ---------------- producers
-    // Thread tid owns the 4 mu columns k4 = (tid % 8) * 4 of every stage and
-    // the nu rows tid / 8 + 16 q (q = 0, 1, 2) of every nu tile: 12
-    // independent gathers of packed D per stage, software-pipelined one stage
-    // ahead as in tc_tile_kernel.  Thread 0 also issues the stage's ten TMA
-    // loads (two blocks x five A planes, 32 x 128 bytes each).
-    const int tid = threadIdx.x;
-    const int k4 = (tid & 7) * 4, nrow0 = tid >> 3;
-    const uint64_t keep = policy_evict_last();
-    int it = 0;
-    int last_issue[kStages];
-#pragma unroll
-    for (int s = 0; s < kStages; ++s) last_issue[s] = -1;
-    for (int i = 0;; ++i) {
-      if (tid == 0) {
-        const int slot = i & 1;
-        int next = -1;
-        if (!mbar_wait(&tile_empty_bar[slot], ((i >> 1) & 1) ^ 1, args.wait_cycles)) {
-          s_abort = 1;
-        } else {
-          const int c = atomicAdd(args.tile_counter, 1);
-          next = c < tb.C ? args.order[c] : -1;
-        }
-        s_tile[slot] = next;
-        mbar_arrive(&tile_full_bar[slot]);
-      }
-      const int t = read_tile_warp(i);
-      if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
-      if (t < 0 || warp_abort()) break;
-      const int kt = tb.kt[t];
-      const int nkb = kt / kBK;
-      const int nnt = (kt + kN - 1) / kN;
-      const int nst = nnt * nkb;
-      const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
-      auto load_idx = [&](int j, int (&nu)[3], int (&mu)[4]) {
-        const int nt = j / nkb, kb = j - nt * nkb;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const int nc = nt * kN + nrow0 + 16 * q;
-          nu[q] = nc < kt ? am[nc] : -1;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) mu[q] = am[kb * kBK + k4 + q];
-      };
-      auto gather = [&](const int (&nu)[3], const int (&mu)[4], uint32_t (&w)[3][4]) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-#pragma unroll
-          for (int m = 0; m < 4; ++m)
-            w[q][m] = (nu[q] >= 0 && mu[m] >= 0)
-                          ? ldg_u32_hint(args.Dp + (int64_t)nu[q] * args.Mpad + mu[m], keep)
-                          : 0u;
-      };
-      int nu[3], mu[4];
-      uint32_t w[3][4];
-      if (nst > 0) {
-        load_idx(0, nu, mu);
-        gather(nu, mu, w);
-      }
-      for (int j = 0; j < nst; ++j, ++it) {
-        const bool more = j + 1 < nst;
-        if (more) load_idx(j + 1, nu, mu);
-        const int s = it % kStages;
-        const uint32_t ph = (it / kStages) & 1;
-        const int k0 = (j % nkb) * kBK;
-        const long long tw = clock64();
-        if (!__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ph ^ 1, args.wait_cycles))) {
-          s_abort = 1;
-          break;
-        }
-        tr0 += clock64() - tw;
-        if (tid == 0) {
-          mbar_arrive_expect_tx(&tma_bar[s], kAStageBytes);
-#pragma unroll
-          for (int h = 0; h < kBlocks; ++h)
-#pragma unroll
-            for (int p = 0; p < kPlanesA; ++p)
-              tma_load_2d_hint(sA + s * kAStageBytes + h * kABlockBytes + p * kAPlaneBytes, &amap, k0,
-                               ((t * kBlocks + h) * kPlanesA + p) * kRows, &tma_bar[s], keep);
-          last_issue[s] = it;
-        }
-        uint8_t* b = sB + s * kBStageBytes;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          uint32_t pl[4];
-          transpose_bytes4x4(w[q][0], w[q][1], w[q][2], w[q][3], pl);
-          const uint32_t off = sw32_offset(nrow0 + 16 * q, k4);
-#pragma unroll
-          for (int p = 0; p < kPlanes; ++p) *(uint32_t*)(b + p * kBPlaneBytes + off) = pl[p];
-        }
-        fence_proxy_async();
-        mbar_arrive(&full_bar[s]);
-        if (more) gather(nu, mu, w);
-      }
-      if (warp_abort()) break;
-    }
-    // every TMA load thread 0 issued has landed before the CTA may exit
-    if (tid == 0) {
-#pragma unroll
-      for (int s = 0; s < kStages; ++s)
-        if (last_issue[s] >= 0 && !mbar_wait(&tma_bar[s], (last_issue[s] / kStages) & 1))
-          atomicExch(args.status, (int32_t)kStatusTimeout);
-    }
-    if (args.trace && tid == 0) {
-      args.trace[(int64_t)blockIdx.x * 8 + 1] = tr0;
-      args.trace[(int64_t)blockIdx.x * 8 + 2] = clock64() - t_start - tr0;
-    }
-  } else if (warp == 4) {
-    // ---------------- MMA issuer
-    // Per stage (one K step of 32) and block h: one MMA per A digit plane pa
-    // against the stage's four D planes read as one B operand of 48 * nb rows
-    // (nb = min(4, 5 - pa)); column block j lands at TMEM column
-    // (5 h + pa + j) * 48, the accumulator of block h and level pa + j.
-    const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kRows >> 4) << 24);
-    int it = 0, gnt = 0;
-    for (int i = 0;; ++i) {
-      const int t = read_tile_warp(i);
-      if (lane == 0) mbar_arrive(&tile_empty_bar[i & 1]);
-      if (t < 0 || warp_abort()) break;
-      const int kt = tb.kt[t];
-      const int nkb = kt / kBK;
-      const int nnt = (kt + kN - 1) / kN;
-      bool failed = false;
-      for (int nt = 0; nt < nnt && !failed; ++nt, ++gnt) {
-        const long long tw = clock64();
-        if (!__all_sync(0xffffffffu, mbar_wait(&tempty_bar, (gnt & 1) ^ 1, args.wait_cycles))) {
-          s_abort = 1;
-          failed = true;
-          break;
-        }
-        tr1 += clock64() - tw;
-        tc_fence_after();
-        for (int kb = 0; kb < nkb; ++kb, ++it) {
-          const int s = it % kStages;
-          const uint32_t ph = (it / kStages) & 1;
-          const long long tf = clock64();
-          const bool ready = mbar_wait(&full_bar[s], ph, args.wait_cycles) &&
-                             mbar_wait(&tma_bar[s], ph, args.wait_cycles);
-          if (!__all_sync(0xffffffffu, ready)) {
-            s_abort = 1;
-            failed = true;
-            break;
-          }
-          tr0 += clock64() - tf;
-          tc_fence_after();
-          if (lane == 0) {
-            const uint32_t a0 = smem_u32(sA + s * kAStageBytes);
-            const uint64_t bd = umma_desc_sw32(smem_u32(sB + s * kBStageBytes));
-#pragma unroll
-            for (int h = 0; h < kBlocks; ++h) {
-#pragma unroll
-              for (int o = 0; o < kPlanesA; ++o) {
-                const int pa = o == 0 ? 0 : (o == 1 ? kPlanesA - 1 : o - 1);  // 0, 4, 1, 2, 3
-                const int nb = kPlanes < kLevels - pa ? kPlanes : kLevels - pa;
-                const uint32_t idesc = idesc0 | ((uint32_t)(nb * kN >> 3) << 17);
-                const uint64_t ad = umma_desc_sw32(a0 + h * kABlockBytes + pa * kAPlaneBytes);
-                umma_i8(tmem + (h * kLevels + pa) * kN, ad, bd, idesc, (kb == 0 && o < 2) ? 0u : 1u);
-              }
-            }
-            umma_commit(&empty_bar[s]);
-          }
-          __syncwarp();
-        }
-        if (failed) break;
-        if (lane == 0) umma_commit(&tfull_bar);
-        __syncwarp();
-      }
-      if (failed || warp_abort()) break;
-    }
-    if (args.trace && lane == 0) {
-      args.trace[(int64_t)blockIdx.x * 8 + 3] = tr0;
-      args.trace[(int64_t)blockIdx.x * 8 + 4] = tr1;
-    }
-  } else {
-    // ---------------- epilogue (warps 5..8 -> TMEM lane quarters 1,2,3,0)
-    // As in tc_tile_kernel, for both blocks: drain this warp's lane quarter of
-    // the ten accumulators (2 blocks x 5 levels) into the FP64 copy of G,
-    // release TMEM, then contract G with the FP64 AO values of the tile's 64
-    // points while the next nu tile's MMAs run.
-    const int quarter = warp & 3;
-    const int role = warp - 5;
-    const int etid = role * 32 + lane;
-    const int nq_ao = tb.nq;
-    const int64_t ldq = (int64_t)tb.TP * tb.Kcap;
-    const uint64_t stream = policy_evict_first();
-    int gnt = 0;
-    bool stop = false;
-    for (int i = 0; !stop; ++i) {
-      if (etid == 0) {
-        s_epi_tile = read_tile(i);
-        mbar_arrive(&tile_empty_bar[i & 1]);
-      }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      const int t = s_epi_tile;
-      if (t < 0) break;
-      const int kt = tb.kt[t];
-      const int nnt = (kt + kN - 1) / kN;
-      const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
-      // AO element (q, k) of point h * 32 + lane at aop[q * ldq + k * 64 + h * 32]
-      const double* aop = tb.ao + (int64_t)t * nq_ao * ldq + lane;
-      double rowscale[kBlocks];
-#pragma unroll
-      for (int h = 0; h < kBlocks; ++h)
-        rowscale[h] = ldexp(1.0, args.eexp[(int64_t)t * kTileRows + h * kRows + quarter * 32 + lane] - 44);
-      double acc[kBlocks][5];
-#pragma unroll
-      for (int h = 0; h < kBlocks; ++h)
-#pragma unroll
-        for (int k = 0; k < 5; ++k) acc[h][k] = 0.0;
-      for (int nt = 0; nt < nnt; ++nt, ++gnt) {
-        const int n0 = nt * kN;
-        double* cs = s_cscale[gnt & 1];
-        if (etid < kN) {
-          const int nc = n0 + etid;
-          const int nu = nc < kt ? am[nc] : -1;
-          cs[etid] = nu >= 0 ? ldexp(1.0, args.fexp[nu]) : 0.0;
-        }
-        // (A) column scales written; every role has finished reading sG
-        asm volatile("bar.sync 1, 128;\n" ::: "memory");
-        if (gnt > 0 && s_epi_abort[(gnt - 1) & 1]) { stop = true; break; }
-        const long long te = clock64();
-        if (!mbar_wait(&tfull_bar, gnt & 1, args.wait_cycles)) s_abort = 1;
-        __syncwarp();  // converged for the .aligned TMEM loads below
-        const long long td = clock64();
-        tr0 += td - te;
-        tc_fence_after();
-#pragma unroll
-        for (int h = 0; h < kBlocks; ++h) {
-          double* gcol = sG + h * kRows + quarter * 32 + lane;
-#pragma unroll 1
-          for (int c = 0; c < kN / 16; ++c) {
-            int32_t v[kLevels][16];
-#pragma unroll
-            for (int L = 0; L < kLevels; ++L)
-              tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (h * kLevels + L) * kN + c * 16, v[L]);
-            tmem_ld_wait();
-#pragma unroll
-            for (int L = 0; L < kLevels; ++L) after_wait16(v[L]);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              double g = i32_times_pow2<0>(v[4][j]);
-              g += i32_times_pow2<8>(v[3][j]);
-              g += i32_times_pow2<16>(v[2][j]);
-              g += i32_times_pow2<24>(v[1][j]);
-              g += i32_times_pow2<32>(v[0][j]);
-              gcol[(c * 16 + j) * kTileRows] = g * rowscale[h] * cs[c * 16 + j];
-            }
-          }
-        }
-        tc_fence_before();
-        mbar_arrive(&tempty_bar);
-        const long long tc0 = clock64();
-        tr1 += tc0 - td;
-        if (etid == 0) s_epi_abort[gnt & 1] = s_abort;
-        // (B) G of this nu tile complete in shared memory
-        asm volatile("bar.sync 1, 128;\n" ::: "memory");
-        const int nvalid = min(kN, kt - n0);  // the last nu tile may end past kt
-#pragma unroll
-        for (int h = 0; h < kBlocks; ++h) {
-          const double* ao_nt = aop + (int64_t)n0 * kPts + h * 32;
-          const double* g_h = sG + h * kRows;
-          switch (role) {
-            case 0: contract_role<0, kEpiGroup, kN, kTileRows, kPts, kPairEpiBuffers>(ao_nt, ldq, g_h, lane, nq_ao, stream, acc[h], nvalid); break;
-            case 1: contract_role<1, kEpiGroup, kN, kTileRows, kPts, kPairEpiBuffers>(ao_nt, ldq, g_h, lane, nq_ao, stream, acc[h], nvalid); break;
-            case 2: contract_role<2, kEpiGroup, kN, kTileRows, kPts, kPairEpiBuffers>(ao_nt, ldq, g_h, lane, nq_ao, stream, acc[h], nvalid); break;
-            default: contract_role<3, kEpiGroup, kN, kTileRows, kPts, kPairEpiBuffers>(ao_nt, ldq, g_h, lane, nq_ao, stream, acc[h], nvalid); break;
-          }
-        }
-        if (args.trace) {
-          double chk = acc[0][0] + acc[1][0];
-          asm volatile("" : "+d"(chk));
-          tr2 += clock64() - tc0;
-        }
-      }
-      // (C) gather the per-point sums and finalise (roles 0 and 1 take one block each)
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      const bool aborted = stop || s_abort != 0;
-#pragma unroll
-      for (int h = 0; h < kBlocks; ++h) {
-        switch (role) {
-          case 0: store_role<0>(s_sums + h * 32, lane, acc[h]); break;
-          case 1: store_role<1>(s_sums + h * 32, lane, acc[h]); break;
-          case 2: store_role<2>(s_sums + h * 32, lane, acc[h]); break;
-          default: store_role<3>(s_sums + h * 32, lane, acc[h]); break;
-        }
-      }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      if (role < kBlocks && !aborted) {
-        const int p = role * 32 + lane;
-        const int64_t pi = (int64_t)t * kPts + p;
-        const int64_t oidx = tb.out[pi];
-        if (oidx >= 0) {
-          if (finite_point(tb.xyz + 3 * pi)) finalize_point(s_sums[p], 4, nq_ao, args.out, oidx, args.prm);
-          else nan_point(args.out, oidx);
-        }
-      }
-    }
-    if (args.trace && etid == 0) {
-      args.trace[(int64_t)blockIdx.x * 8 + 5] = tr0;
-      args.trace[(int64_t)blockIdx.x * 8 + 6] = tr1;
-      args.trace[(int64_t)blockIdx.x * 8 + 7] = tr2;
-    }
-  }
-  __syncthreads();
-  if (args.trace && threadIdx.x == 0) args.trace[(int64_t)blockIdx.x * 8] = clock64() - t_start;
-  if (s_abort && threadIdx.x == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
-  if (warp == 4) {
-    if (lane == 0) umma_commit(&done_bar);
-    __syncwarp();
-    if (!mbar_wait(&done_bar, 0) && lane == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
-    __syncwarp();  // converged for the .aligned dealloc
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
-  }
-}
-
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -1280,9 +846,9 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
   CTC_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
   if (major != 10) return fail(CTC_ERR_UNSUPPORTED, "tensor-core split path needs an sm_100 GPU");
   const size_t MM = (size_t)mol->Mpad * mol->Mpad;
-  if (!mol->d_Dsl) CTC_CUDA_TRY(cudaMalloc((void**)&mol->d_Dsl, sizeof(uint32_t) * MM));
+  if (!mol->d_Dsl) CTC_CUDA_TRY(cudaMalloc((void**)&mol->d_Dsl, sizeof(uint64_t) * MM));
   if (!mol->d_Dscale) CTC_CUDA_TRY(cudaMalloc((void**)&mol->d_Dscale, sizeof(int32_t) * mol->Mpad));
-  slice_d_kernel<<<mol->Mpad, 256, 0, st>>>(mol->d_D, mol->Mpad, (uint32_t*)mol->d_Dsl,
+  slice_d_kernel<<<mol->Mpad, 256, 0, st>>>(mol->d_D, mol->Mpad, (uint64_t*)mol->d_Dsl,
                                             (int32_t*)mol->d_Dscale);
   CTC_CUDA_TRY(cudaGetLastError());
   mol->dsl_valid = true;
@@ -1381,27 +947,22 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   // int8 planes of the tile rows, row exponents and the tile order (largest
   // compact K first, zeroed tile counter), written for this chunk by
   // tc_slice_workspace and the AO kernel (launch_ao_tiles_sliced)
-  // 64-point tiles of phi and grad phi rows run on tc_pair_kernel, 128-point
-  // tiles of phi rows on tc_tile_kernel<1>
-  const bool paired = plan.nqa == 4;
-  if (paired ? tb.TP != pair::kPts : !(plan.nqa == 1 && tb.TP == 128))
+  if (!((plan.nqa == 4 && tb.TP == 32) || (plan.nqa == 1 && tb.TP == 128)))
     return fail(CTC_ERR_INVALID, "tensor-core split path: unsupported tile layout");
   const int rows = split_tile_rows(tb.TP, plan.nqa);
   TcWorkspace w;
   if ((rc = tc_workspace(mol, tb, rows, st, &w)) != CTC_OK) return rc;
   // tensor map over the planes: 2-D, rows = C * rows * 5, inner = Kcap bytes;
-  // boxes of 32 (pair kernel, 32-byte swizzle) or 64 bytes (64-byte swizzle)
-  // by 128 rows
+  // boxes of 64 bytes (64-byte swizzle) by 128 rows
   PFN_cuTensorMapEncodeTiled_v12000 enc = get_encode();
   if (!enc) return fail(CTC_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   CUtensorMap amap;
   cuuint64_t gdim[2] = {(cuuint64_t)tb.Kcap, (cuuint64_t)tb.C * kPlanesA * rows};
   cuuint64_t gstride[1] = {(cuuint64_t)tb.Kcap};
-  cuuint32_t box[2] = {(cuuint32_t)(paired ? pair::kBK : kBK), (cuuint32_t)kRows};
+  cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kRows};
   cuuint32_t estr[2] = {1, 1};
   CUresult cr = enc(&amap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, w.planes, gdim, gstride, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    paired ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return fail(CTC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)cr));
   int num_sms = 0;
@@ -1410,7 +971,7 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   TcArgs a;
   a.tb = tb;
   a.nqa = plan.nqa;
-  a.Dp = (const uint32_t*)mol->d_Dsl;
+  a.Dp = (const uint64_t*)mol->d_Dsl;
   a.fexp = (const int32_t*)mol->d_Dscale;
   a.eexp = w.eexp;
   a.Mpad = mol->Mpad;
@@ -1425,11 +986,11 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   // on stderr after each launch (synchronises the stream; diagnostics only)
   static const bool trace_on = std::getenv("CTC_TC_TRACE") != nullptr;
   if (trace_on) CTC_CUDA_TRY(cudaMallocAsync((void**)&a.trace, sizeof(long long) * 8 * grid, st));
-  if ((rc = paired ? ensure_smem_attr((const void*)tc_pair_kernel, pair::kSmem)
-                   : ensure_smem_attr((const void*)tc_tile_kernel<1>, kSmemTc)) != CTC_OK)
+  if ((rc = ensure_smem_attr(plan.nqa == 4 ? (const void*)tc_tile_kernel<4> : (const void*)tc_tile_kernel<1>,
+                             kSmemTc)) != CTC_OK)
     return rc;
   ProfScope ps(mol, 0, st);
-  if (paired) tc_pair_kernel<<<grid, kThreadsTc, pair::kSmem, st>>>(amap, a);
+  if (plan.nqa == 4) tc_tile_kernel<4><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
   else tc_tile_kernel<1><<<grid, kThreadsTc, kSmemTc, st>>>(amap, a);
   CTC_CUDA_TRY(cudaGetLastError());
   if (trace_on) {
@@ -1444,9 +1005,8 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
       for (int k = 0; k < 8; ++k) sum[k] += (double)tr[(size_t)8 * i + k];
       totmax = std::max(totmax, (double)tr[(size_t)8 * i]);
     }
-    const int sbk = paired ? pair::kBK : kBK, sn = paired ? pair::kN : kN;
     for (int i = 0; i < tb.C; ++i) {
-      stages += (kt[i] / (double)sbk) * std::ceil(kt[i] / (double)sn);
+      stages += (kt[i] / (double)kBK) * std::ceil(kt[i] / (double)kN);
       ktsum += kt[i];
       ktmax = std::max(ktmax, (double)kt[i]);
     }

@@ -46,7 +46,7 @@ extern "C" {
 
 /* ---- precision of the Phi*D contraction ------------------------------------------------------ */
 #define CTC_PREC_FP64 0      /* FP64 throughout (double-precision matrix units) */
-#define CTC_PREC_TC_SPLIT 1  /* INT8 tensor cores, operands split into int8 digits (5 for the AO rows, 4 for D), exact int32 accumulation */
+#define CTC_PREC_TC_SPLIT 1  /* INT8 tensor cores, operands split into int8 digits (5 for the AO rows, 5 for D), exact int32 accumulation */
 
 typedef struct ctc_molecule ctc_molecule; /* opaque handle */
 

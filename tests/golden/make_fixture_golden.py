@@ -23,7 +23,9 @@ those molecules, in two phases:
 DIR defaults to $CTC_REFERENCE/tests/data (CTC_REFERENCE: the reference's
 checkout).  Drivers that refuse a molecule (the reference's ESP needs the whole
 basis in its constant-memory array and has no g functions) are skipped and
-listed in meta_skipped.
+listed in meta_skipped; the ESP is not called at all for bases with g
+functions, which the reference's ESP does not support (its kernel stops on a
+device-side assert there).
 """
 from __future__ import annotations
 
@@ -105,8 +107,14 @@ def run_reference(out_dir: str) -> int:
         rec = dict(np.load(inp))
         rec = {k: v for k, v in rec.items() if not k.startswith("ref_")}
         skipped = []
+        # The reference's ESP has no g functions (src/evaluate_electrostatic.cu:10135-10137);
+        # called on a basis with g shells its kernel stops on a device-side assert, so it is
+        # never called for one.
+        funcs = [f for f in FUNCS if not (f == "esp" and np.any(np.abs(rec["in_angmoms"]) >= 4))]
+        if len(funcs) < len(FUNCS):
+            skipped.append("esp: not run, the reference's ESP has no g functions")
         with tempfile.TemporaryDirectory() as td:
-            for fn in FUNCS:
+            for fn in funcs:
                 path = os.path.join(td, fn + ".npy")
                 r = subprocess.run([sys.executable, os.path.abspath(__file__), "one", inp, fn, path],
                                    capture_output=True, text=True, timeout=300)
