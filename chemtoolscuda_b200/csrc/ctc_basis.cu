@@ -462,6 +462,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   cudaFree(m->d_ao_perm);
   cudaFree(m->d_Dsl);
   cudaFree(m->d_Dscale);
+  cudaFree(m->d_nzpair);
   cudaFree(m->d_status);
   if (m->h_status) cudaFreeHost(m->h_status);
   if (m->status_ev) cudaEventDestroy(m->status_ev);

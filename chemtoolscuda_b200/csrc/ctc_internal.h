@@ -159,6 +159,11 @@ struct ctc_molecule {
   int8_t* d_Dsl = nullptr;
   double* d_Dscale = nullptr;
   bool dsl_valid = false;
+  // atom pairs with a non-zero block of D (natom x natom bytes), built with
+  // the split copy when some atom-pair block of D is zero (a cut-off density
+  // matrix); the tensor-core kernel then skips the K stages of tiles whose
+  // D block is entirely zero.  nullptr: every block is taken.
+  uint8_t* d_nzpair = nullptr;
   // status word written by kernels (sticky until reported), its pinned host
   // copy ([0]; [1] receives the capacity pre-pass's count), and the event
   // recorded after the copy was enqueued

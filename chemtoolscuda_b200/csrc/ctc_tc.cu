@@ -372,6 +372,59 @@ __global__ void slice_d_kernel(const double* __restrict__ D, int Mpad, uint64_t*
     Dp[(int64_t)row * Mpad + k] = pack_digits5(rint_i64(d[k] * f));
 }
 
+// Atom pairs with a non-zero element of D: nz[a * natom + b] = 1 for every
+// D[mu][nu] != 0 with mu on atom a, nu on atom b (internal AO order).
+__global__ void atom_pair_nonzero_kernel(const double* __restrict__ D, int M, int Mpad,
+                                         const int32_t* __restrict__ ao_atom, int natom,
+                                         uint8_t* __restrict__ nz) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)M * M) return;
+  const int i = (int)(e / M), j = (int)(e % M);
+  if (D[(int64_t)i * Mpad + j] != 0.0) nz[(int64_t)ao_atom[i] * natom + ao_atom[j]] = 1;
+}
+
+// Active K stages of each tile: bit nt * nb + kb of tile t's mask is set when
+// the D block of nu block nt and mu block kb (64 compact AOs each) has a
+// non-zero atom pair, and always for kb = 0 (the stage that initialises the
+// accumulators of a nu tile).  One block per tile; a 64-AO block with more
+// than kMaskAtoms distinct atoms is taken as non-zero.
+constexpr int kMaskAtoms = 16;
+__global__ void __launch_bounds__(256)
+    stage_mask_kernel(TileBatch tb, const int32_t* __restrict__ ao_atom, const uint8_t* __restrict__ nz,
+                      int natom, uint32_t* __restrict__ mask, int mask_words) {
+  __shared__ int s_at[256][kMaskAtoms + 1];  // per 64-AO block: count, then atoms
+  const int t = blockIdx.x;
+  const int nb = tb.kt[t] / 64;
+  const int32_t* am = tb.aomap + (int64_t)t * tb.Kcap;
+  uint32_t* mk = mask + (int64_t)t * mask_words;
+  for (int w = threadIdx.x; w < mask_words; w += blockDim.x) mk[w] = 0u;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    int cnt = 0;
+    for (int k = 0; k < 64 && cnt <= kMaskAtoms; ++k) {
+      const int ao = am[b * 64 + k];
+      if (ao < 0) continue;
+      const int a = ao_atom[ao];
+      bool seen = false;
+      for (int i = 0; i < cnt && i < kMaskAtoms; ++i) seen |= s_at[b][1 + i] == a;
+      if (!seen) {
+        if (cnt < kMaskAtoms) s_at[b][1 + cnt] = a;
+        ++cnt;
+      }
+    }
+    s_at[b][0] = cnt;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int bi = e / nb, bj = e % nb;  // nu block, mu block
+    bool on = bj == 0;
+    const int ci = s_at[bi][0], cj = s_at[bj][0];
+    if (ci > kMaskAtoms || cj > kMaskAtoms) on = true;
+    for (int i = 0; i < ci && !on; ++i)
+      for (int j = 0; j < cj && !on; ++j) on = nz[(int64_t)s_at[bi][1 + i] * natom + s_at[bj][1 + j]] != 0;
+    if (on) atomicOr(&mk[e >> 5], 1u << (e & 31));
+  }
+}
+
 // ------------------------------------------------------------------ main kernel
 struct TcArgs {
   TileBatch tb;
@@ -390,6 +443,10 @@ struct TcArgs {
   // limit of every pipeline wait, in SM cycles (kWaitCycles unless a caller
   // shortens it to exercise the timeout path)
   long long wait_cycles;
+  // active K stages per tile (stage_mask_kernel), mask_words words per tile;
+  // nullptr: every stage is active
+  const uint32_t* stage_mask;
+  int mask_words;
   // optional per-CTA cycle counters (CTC_TC_TRACE): [grid][8] = total,
   // producer wait on empty, producer stage work, MMA wait on full, MMA wait
   // on tempty, epilogue wait on tfull, drain, contraction
@@ -476,6 +533,11 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     return __shfl_sync(0xffffffffu, t, 0);
   };
   auto warp_abort = [&]() -> bool { return __any_sync(0xffffffffu, s_abort != 0); };
+  // is stage j (= nu tile * nkb + K block) of tile t active?  (block-sparse D)
+  auto stage_on = [&](int t, int j) -> bool {
+    return !args.stage_mask ||
+           ((__ldg(args.stage_mask + (int64_t)t * args.mask_words + (j >> 5)) >> (j & 31)) & 1u);
+  };
 
   if (warp < 4) {
     // ---------------- producers
@@ -535,13 +597,20 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       };
       int nu[8], mu[4];
       uint64_t w[8][4];
-      if (nst > 0) {
-        load_idx(0, nu, mu);
+      // the tile's active stages in order (every stage unless D is block-sparse)
+      auto next_on = [&](int j) -> int {
+        while (j < nst && !stage_on(t, j)) ++j;
+        return j;
+      };
+      int j = next_on(0);
+      if (j < nst) {
+        load_idx(j, nu, mu);
         gather(nu, mu, w);
       }
-      for (int j = 0; j < nst; ++j, ++it) {
-        const bool more = j + 1 < nst;
-        if (more) load_idx(j + 1, nu, mu);
+      for (; j < nst; ++it) {
+        const int jn = next_on(j + 1);
+        const bool more = jn < nst;
+        if (more) load_idx(jn, nu, mu);
         const int s = it % kStages;
         const uint32_t ph = (it / kStages) & 1;
         const int k0 = (j % nkb) * kBK;
@@ -578,6 +647,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         fence_proxy_async();
         mbar_arrive(&full_bar[s]);
         if (more) gather(nu, mu, w);
+        j = jn;
       }
       if (warp_abort()) break;
     }
@@ -625,7 +695,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
         }
         tr1 += clock64() - tw;
         tc_fence_after();
-        for (int kb = 0; kb < nkb; ++kb, ++it) {
+        for (int kb = 0; kb < nkb; ++kb) {
+          if (!stage_on(t, nt * nkb + kb)) continue;  // zero D block: no data, no MMA
           const int s = it % kStages;
           const uint32_t ph = (it / kStages) & 1;
           const long long tf = clock64();
@@ -661,6 +732,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
             umma_commit(&empty_bar[s]);
           }
           __syncwarp();
+          ++it;
         }
         if (failed) break;
         if (lane == 0) umma_commit(&tfull_bar);
@@ -851,6 +923,29 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
   slice_d_kernel<<<mol->Mpad, 256, 0, st>>>(mol->d_D, mol->Mpad, (uint64_t*)mol->d_Dsl,
                                             (int32_t*)mol->d_Dscale);
   CTC_CUDA_TRY(cudaGetLastError());
+  // atom-pair map of D's non-zero blocks, kept only if some block is zero
+  // (every AO on an atom, at most 4096 atoms: a map of 16 MB at most)
+  cudaFree(mol->d_nzpair);
+  mol->d_nzpair = nullptr;
+  const int na = mol->natom;
+  bool atoms_ok = na > 0 && na <= 4096;
+  for (int a : mol->ao_atom) atoms_ok = atoms_ok && a >= 0 && a < na;
+  if (atoms_ok) {
+    const size_t nn = (size_t)na * na;
+    CTC_CUDA_TRY(cudaMalloc((void**)&mol->d_nzpair, nn));
+    CTC_CUDA_TRY(cudaMemsetAsync(mol->d_nzpair, 0, nn, st));
+    const int64_t MM2 = (int64_t)mol->M * mol->M;
+    atom_pair_nonzero_kernel<<<(unsigned)((MM2 + 255) / 256), 256, 0, st>>>(
+        mol->d_D, mol->M, mol->Mpad, mol->d_ao_atom, na, mol->d_nzpair);
+    CTC_CUDA_TRY(cudaGetLastError());
+    std::vector<uint8_t> h(nn);
+    CTC_CUDA_TRY(cudaMemcpyAsync(h.data(), mol->d_nzpair, nn, cudaMemcpyDeviceToHost, st));
+    CTC_CUDA_TRY(cudaStreamSynchronize(st));
+    if (std::find(h.begin(), h.end(), (uint8_t)0) == h.end()) {  // dense: nothing to skip
+      cudaFree(mol->d_nzpair);
+      mol->d_nzpair = nullptr;
+    }
+  }
   mol->dsl_valid = true;
   return CTC_OK;
 }
@@ -863,6 +958,8 @@ int prepare_tc(ctc_molecule* mol, cudaStream_t st) {
 struct TcWorkspace {
   int8_t* planes;
   int32_t* eexp;
+  uint32_t* mask;  // active K stages per tile (mask_words each), block-sparse D only
+  int mask_words;
   uint32_t* keys_in;
   uint32_t* keys_out;
   int32_t* ids;
@@ -885,6 +982,9 @@ int tc_workspace(ctc_molecule* mol, const TileBatch& tb, int rows, cudaStream_t 
   };
   const size_t o_planes = take((size_t)tb.C * kPlanesA * rows * tb.Kcap);
   const size_t o_eexp = take(sizeof(int32_t) * (size_t)tb.C * rows);
+  const int nbmax = tb.Kcap / kBK;
+  const int mask_words = mol->d_nzpair ? (nbmax * nbmax + 31) / 32 : 0;
+  const size_t o_mask = take(sizeof(uint32_t) * (size_t)tb.C * mask_words);
   const size_t o_kin = take(sizeof(uint32_t) * tb.C);
   const size_t o_kout = take(sizeof(uint32_t) * tb.C);
   const size_t o_ids = take(sizeof(int32_t) * tb.C);
@@ -896,6 +996,8 @@ int tc_workspace(ctc_molecule* mol, const TileBatch& tb, int rows, cudaStream_t 
   char* base = (char*)mol->ws_sl.p;
   w->planes = (int8_t*)(base + o_planes);
   w->eexp = (int32_t*)(base + o_eexp);
+  w->mask = mask_words ? (uint32_t*)(base + o_mask) : nullptr;
+  w->mask_words = mask_words;
   w->keys_in = (uint32_t*)(base + o_kin);
   w->keys_out = (uint32_t*)(base + o_kout);
   w->ids = (int32_t*)(base + o_ids);
@@ -982,6 +1084,14 @@ int tc_local_tiles(ctc_molecule* mol, const LocalPlan& plan, const TileBatch& tb
   a.tile_counter = w.counter;
   a.trace = nullptr;
   a.wait_cycles = mol->wait_cycles > 0 ? (long long)mol->wait_cycles : kWaitCycles;
+  a.stage_mask = w.mask;
+  a.mask_words = w.mask_words;
+  if (w.mask) {
+    stage_mask_kernel<<<tb.C, 256, 0, st>>>(tb, mol->d_ao_atom, mol->d_nzpair, mol->natom, w.mask,
+                                           w.mask_words);
+    CTC_CUDA_TRY(cudaGetLastError());
+    mol->host_launches += 1;
+  }
   // CTC_TC_TRACE=1: per-CTA cycle counters of the kernel's roles, summarised
   // on stderr after each launch (synchronises the stream; diagnostics only)
   static const bool trace_on = std::getenv("CTC_TC_TRACE") != nullptr;
