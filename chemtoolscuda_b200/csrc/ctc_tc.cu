@@ -262,17 +262,13 @@ __device__ __forceinline__ constexpr int role_sum(int role, int slot, int row) {
 // columns)
 constexpr int kEpiGroup = 2;
 
-// COLS columns per nu tile, GS doubles between the columns of sG, PS points
-// between consecutive AO columns of one quantity in the AO block.  Only the
-// first nvalid columns of the nu tile lie inside the tile's compact AO range;
-// loads of the others read column nvalid - 1 instead (their G is zero).
-template <int ROLE, int GW, int COLS = kN, int GS = kRows, int PS = 32, int NB = 16 / GW>
+template <int ROLE, int GW>
 __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int64_t ldq,
                                               const double* __restrict__ sG, int lane, int nq_ao,
-                                              uint64_t stream, double* acc, int nvalid = COLS) {
+                                              uint64_t stream, double* acc) {
   constexpr int NS = role_nslot(ROLE);
-  constexpr int NG = COLS / GW;  // groups of GW columns
-  // NB register buffers of one group each
+  constexpr int NG = kN / GW;    // groups of GW columns
+  constexpr int NB = 16 / GW;    // register buffers of one group each
   bool live[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) live[s] = role_q(ROLE, s) < nq_ao;
@@ -284,7 +280,7 @@ __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int
     for (int s = 0; s < NS; ++s)
 #pragma unroll
       for (int j = 0; j < GW; ++j)
-        a[buf][s][j] = live[s] ? ldg_f64_stream(ao + role_q(ROLE, s) * ldq + min(cg + j, nvalid - 1) * PS, stream) : 0.0;
+        a[buf][s][j] = live[s] ? ldg_f64_stream(ao + role_q(ROLE, s) * ldq + (cg + j) * 32, stream) : 0.0;
   };
 #pragma unroll
   for (int g = 0; g < NB - 1; ++g) load(g, g * GW);
@@ -294,7 +290,7 @@ __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int
     const int cg = g * GW;
 #pragma unroll
     for (int j = 0; j < GW; ++j) {
-      const double* gp = sG + (cg + j) * GS + lane;
+      const double* gp = sG + (cg + j) * kRows + lane;
       int i = 0;
 #pragma unroll
       for (int s = 0; s < NS; ++s)

@@ -593,9 +593,8 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
                      cudaStream_t st, const std::function<int(const TileBatch&)>& compute,
                      const std::function<int(const TileBatch&)>* ao_launch = nullptr,
                      int rows = 128) {
-  // cubic-grid tiles: blocks of 2x4x4, 4x4x4 or 4x4x8 grid points
+  // cubic-grid tiles: blocks of 2x4x4 or 4x4x8 grid points
   int TX = 2, TY = 4, TZ = 4;
-  if (TP == 64) { TX = 4; TY = 4; TZ = 4; }
   if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
   int64_t ntiles, nbx = 0, nby = 0, nbz = 0;
   int nx = 0;
