@@ -410,8 +410,11 @@ static int build_esp(ctc_molecule* mol) {
     }
     for (size_t l = 0; l < outs.size(); ++l) {
       size_t w = 0;
-      for (size_t i = 0; i < outs[l].size(); ++i)
-        if (!drop[l][i]) outs[l][w++] = std::move(outs[l][i]);
+      for (size_t i = 0; i < outs[l].size(); ++i) {
+        if (drop[l][i]) continue;
+        if (w != i) outs[l][w] = std::move(outs[l][i]);  // a self-move would empty h
+        ++w;
+      }
       outs[l].resize(w);
     }
   }
