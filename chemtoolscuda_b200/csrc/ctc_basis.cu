@@ -472,6 +472,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   m->ws_part.release();
   m->ws_misc.release();
   m->ws_cap.release();
+  m->ws_esp.release();
   if (m->hostpipe) {
     m->hostpipe->release();
     delete m->hostpipe;

@@ -12,12 +12,18 @@
 // depends on the point only through R, the Hermite densities h are built once
 // per molecule (host, all cores) and each point costs one Boys evaluation and
 // one R recursion per significant primitive pair -- no integral matrix.
+// Pairs are grouped by L = l_a + l_b; each class runs as its own kernel
+// (registers sized for its L), over a 2-D grid of 128-point blocks x slices
+// of the class's pairs.
 //
-// Boys function F_n(T) (FP64): for T < 40 a 7-term Taylor expansion about the
-// nearest point of a 0.05-spaced table gives F_L, and F_{n-1} = (2T F_n +
-// e^{-T})/(2n-1) (downward recursion, stable) gives the rest; for T >= 40,
-// F_0 = sqrt(pi/T)/2 and upward recursion (stable there).  The table is built
-// at set-up from the series F_m(T) = e^{-T} sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
+// Boys function F_n(T) (FP64): beyond a per-L threshold (T >= 38 + 3L, where
+// the neglected e^{-T} terms are below 2e-17 relative) the asymptotic forms
+// hold -- a far pair is a point multipole and costs one rsqrt and no
+// exponential; 99% of (point, pair) evaluations on molecular surfaces are of
+// this kind.  Below it, a 7-term Taylor expansion about the nearest point of
+// a 0.05-spaced table gives F_L, and F_{n-1} = (2T F_n + e^{-T})/(2n-1)
+// (downward recursion, stable) gives the rest.  The table is built at set-up
+// from the series F_m(T) = e^{-T} sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)).
 // (The reference uses forward recursion from erf, include/boys_functions.cuh:13-31,
 // which loses digits at small T and divides by zero at T = 0.)
 //
@@ -44,7 +50,7 @@ constexpr int kLmax = 8;                 // g x g
 constexpr int kTaylor = 7;               // terms of the Taylor expansion
 constexpr int kNF = kLmax + kTaylor;     // orders stored per table point
 constexpr double kTstep = 0.05;
-constexpr double kTmax = 40.0;
+constexpr double kTmax = 64.0;           // table range: above every far_T(L <= 8)
 constexpr int kNT = (int)(kTmax / kTstep) + 2;
 constexpr double kPi = 3.14159265358979323846;
 
@@ -59,7 +65,9 @@ __host__ __device__ constexpr int tuv_index(int t, int u, int v) {
 }
 
 struct EspPair {
-  double Px, Py, Pz, p, pref;  // pref = 2 pi / p
+  double Px, Py, Pz, p;
+  double f0c;  // sqrt(pi / p) / 2: F_0 = f0c / |P - C| in the far field
+  double pad;
 };
 struct EspBatch {
   int32_t b0, b1;   // pairs [b0, b1)
@@ -79,6 +87,13 @@ double boys_series(int m, double T) {
 
 }  // namespace
 
+// pairs per batch of class L (a batch's Hermite coefficients fit 32 KB)
+constexpr int kBatchPairs = 64;
+constexpr int kBatchH = 4096;
+__host__ __device__ constexpr int batch_pairs(int L) {
+  return kBatchPairs < kBatchH / ntuv(L) ? kBatchPairs : kBatchH / ntuv(L);
+}
+
 struct EspTables {
   double* d_boys = nullptr;
   EspPair* d_pairs = nullptr;
@@ -86,6 +101,7 @@ struct EspTables {
   EspBatch* d_batches = nullptr;
   double* d_atoms = nullptr;  // x y z Z per atom
   int npairs = 0, nbatch = 0, natom = 0;
+  int lb0[kLmax + 2] = {};  // batches of class L: [lb0[L], lb0[L + 1])
   size_t nh = 0;
   // algorithmic FP64 work per point: sum over the kept pairs of
   // 2 n_tuv(L) (contraction) + 2 n_R(L) (R recursion) + 10 (L + 1) (Boys)
@@ -96,36 +112,54 @@ struct EspTables {
 namespace {
 
 // ------------------------------------------------------------------ device side
+// First T from which the asymptotic forms F_0 = sqrt(pi/T)/2, F_n =
+// (2n-1)/(2T) F_{n-1} agree with F_n(T) to 2e-17 relative for every n <= L
+// (the neglected terms are e^{-T} and erfc(sqrt T); thresholds checked against
+// the incomplete-gamma form of F_n in 40-digit arithmetic: 37, 41, 44, 47, 50,
+// 53, 55, 58, 60 for L = 0..8).
+__host__ __device__ constexpr double far_T(int L) { return 38.0 + 3.0 * L; }
+
+// G_n = R^n_000 = (-2p)^n F_n(T), n = 0..L, at T = p r2.
+//  far field (T >= far_T(L)): the p dependence cancels except in F_0,
+//    G_0 = (sqrt(pi/p)/2) / r,  G_n = -(2n-1) G_{n-1} / r2  -- no exponential;
+//  otherwise: F_L from the 7-term Taylor table about the nearest 0.05 step,
+//    F_{n-1} = (2T F_n + e^{-T}) / (2n-1) downwards (stable for every T).
 template <int L>
-__device__ __forceinline__ void boys(double T, const double* __restrict__ tab, double* F) {
-  const double e = exp(-T);
-  if (T < kTmax) {
+__device__ __forceinline__ void boys_g(double p, double f0c, double r2, const double* __restrict__ tab,
+                                       double* G) {
+  const double T = p * r2;
+  if (T >= far_T(L)) {
+    const double ri = rsqrt(r2);
+    const double ri2 = ri * ri;
+    G[0] = f0c * ri;
+#pragma unroll
+    for (int n = 1; n <= L; ++n) G[n] = -(double)(2 * n - 1) * ri2 * G[n - 1];
+  } else {
+    const double e = exp(-T);
     const int i = __double2int_rn(T * (1.0 / kTstep));
     const double d = i * kTstep - T;  // -(T - T_i)
     const double* row = tab + i * kNF + L;
+    double F[L + 1];
     double fl = row[kTaylor - 1];
 #pragma unroll
-    for (int k = kTaylor - 2; k >= 0; --k) fl = row[k] + fl * d / (double)(k + 1);
+    for (int k = kTaylor - 2; k >= 0; --k) fl = row[k] + fl * d * (1.0 / (double)(k + 1));
     F[L] = fl;
 #pragma unroll
-    for (int n = L; n > 0; --n) F[n - 1] = (2.0 * T * F[n] + e) / (2 * n - 1);
-  } else {
-    F[0] = 0.5 * sqrt(kPi / T);
-    const double inv2T = 0.5 / T;
+    for (int n = L; n > 0; --n) F[n - 1] = (2.0 * T * F[n] + e) * (1.0 / (double)(2 * n - 1));
+    double m = 1.0;
 #pragma unroll
-    for (int n = 1; n <= L; ++n) F[n] = ((2 * n - 1) * F[n - 1] - e) * inv2T;
+    for (int n = 0; n <= L; ++n) {
+      G[n] = m * F[n];
+      m *= -2.0 * p;
+    }
   }
 }
 
-// R^0_{tuv}(p, X, Y, Z) for t+u+v <= L, in place from level L down to 0.
+// R^0_{tuv}(p, X, Y, Z) for t+u+v <= L, in place from level L down to 0,
+// from G_n = R^n_000.
 template <int L>
-__device__ __forceinline__ void hermite_r(double p, double X, double Y, double Z, const double* F,
-                                          double* R) {
-  double m2p[L + 1];
-  m2p[0] = 1.0;
-#pragma unroll
-  for (int n = 1; n <= L; ++n) m2p[n] = m2p[n - 1] * (-2.0 * p);
-  R[0] = m2p[L] * F[L];
+__device__ __forceinline__ void hermite_r(double X, double Y, double Z, const double* G, double* R) {
+  R[0] = G[L];
 #pragma unroll
   for (int n = L - 1; n >= 0; --n) {
     // level n: totals L-n down to 1 from level n+1, then total 0
@@ -151,43 +185,28 @@ __device__ __forceinline__ void hermite_r(double p, double X, double Y, double Z
         }
       }
     }
-    R[0] = m2p[n] * F[n];
+    R[0] = G[n];
   }
-}
-
-template <int L>
-__device__ __forceinline__ double esp_batch(const EspPair* sp, const double* sh, int np, double cx,
-                                            double cy, double cz, const double* __restrict__ tab) {
-  constexpr int NT = ntuv(L);
-  double acc = 0.0;
-  for (int i = 0; i < np; ++i) {
-    const EspPair q = sp[i];
-    const double X = q.Px - cx, Y = q.Py - cy, Z = q.Pz - cz;
-    const double T = q.p * (X * X + Y * Y + Z * Z);
-    double F[L + 1];
-    boys<L>(T, tab, F);
-    double R[NT];
-    hermite_r<L>(q.p, X, Y, Z, F, R);
-    const double* h = sh + i * NT;
-    double s = 0.0;
-#pragma unroll
-    for (int k = 0; k < NT; ++k) s += h[k] * R[k];
-    acc += q.pref * s;
-  }
-  return acc;
 }
 
 constexpr int kEspThreads = 128;
-constexpr int kBatchPairs = 64;
-constexpr int kBatchH = 4096;
 
+// Electronic ESP of the pairs of one angular class L: block (x, y) takes 128
+// points and slice y of the class's batches and writes its partial sum
+// sum_pairs sum_tuv h_tuv R_tuv (h already carries 2 pi / p) to row y of
+// part.  Rows are summed in a fixed order by esp_finish_kernel, so results do
+// not depend on the launch shape's timing.
+template <int L>
 __global__ void __launch_bounds__(kEspThreads)
-    esp_kernel(const EspPair* __restrict__ pairs, const double* __restrict__ hbuf,
-               const EspBatch* __restrict__ batches, int nbatch, const double* __restrict__ tab,
-               const double* __restrict__ atoms, int natom, const double* __restrict__ pts,
-               int64_t n, double* __restrict__ out) {
-  __shared__ EspPair sp[kBatchPairs];
-  __shared__ double sh[kBatchH];
+    esp_class_kernel(const EspPair* __restrict__ pairs, const double* __restrict__ hbuf,
+                     const EspBatch* __restrict__ batches, int b0, int nb, const double* __restrict__ tab,
+                     const double* __restrict__ pts, int64_t n, double* __restrict__ part) {
+  constexpr int NT = ntuv(L);
+  constexpr int BP = batch_pairs(L);
+  __shared__ EspPair sp[BP];
+  __shared__ double sh[BP * NT];
+  const int slices = gridDim.y, y = blockIdx.y;
+  const int bb = b0 + (int)((int64_t)nb * y / slices), be = b0 + (int)((int64_t)nb * (y + 1) / slices);
   const int64_t ip = (int64_t)blockIdx.x * kEspThreads + threadIdx.x;
   const bool live = ip < n;
   double cx = 0, cy = 0, cz = 0;
@@ -196,29 +215,41 @@ __global__ void __launch_bounds__(kEspThreads)
     cy = pts[3 * ip + 1];
     cz = pts[3 * ip + 2];
   }
-  double elec = 0.0;
-  for (int b = 0; b < nbatch; ++b) {
+  double acc = 0.0;
+  for (int b = bb; b < be; ++b) {
     const EspBatch bt = batches[b];
     const int np = bt.b1 - bt.b0;
-    const int nh = np * ntuv(bt.L);
     __syncthreads();
     for (int i = threadIdx.x; i < np; i += kEspThreads) sp[i] = pairs[bt.b0 + i];
-    for (int i = threadIdx.x; i < nh; i += kEspThreads) sh[i] = hbuf[bt.h0 + i];
+    for (int i = threadIdx.x; i < np * NT; i += kEspThreads) sh[i] = hbuf[bt.h0 + i];
     __syncthreads();
     if (!live) continue;
-    switch (bt.L) {
-      case 0: elec += esp_batch<0>(sp, sh, np, cx, cy, cz, tab); break;
-      case 1: elec += esp_batch<1>(sp, sh, np, cx, cy, cz, tab); break;
-      case 2: elec += esp_batch<2>(sp, sh, np, cx, cy, cz, tab); break;
-      case 3: elec += esp_batch<3>(sp, sh, np, cx, cy, cz, tab); break;
-      case 4: elec += esp_batch<4>(sp, sh, np, cx, cy, cz, tab); break;
-      case 5: elec += esp_batch<5>(sp, sh, np, cx, cy, cz, tab); break;
-      case 6: elec += esp_batch<6>(sp, sh, np, cx, cy, cz, tab); break;
-      case 7: elec += esp_batch<7>(sp, sh, np, cx, cy, cz, tab); break;
-      default: elec += esp_batch<8>(sp, sh, np, cx, cy, cz, tab); break;
+    for (int i = 0; i < np; ++i) {
+      const EspPair q = sp[i];
+      const double X = q.Px - cx, Y = q.Py - cy, Z = q.Pz - cz;
+      double G[L + 1];
+      boys_g<L>(q.p, q.f0c, X * X + Y * Y + Z * Z, tab, G);
+      double R[NT];
+      hermite_r<L>(X, Y, Z, G, R);
+      const double* h = sh + i * NT;
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NT; ++k) s += h[k] * R[k];
+      acc += s;
     }
   }
-  if (!live) return;
+  if (live) part[(int64_t)y * n + ip] = acc;
+}
+
+// V = sum_A Z_A / |C - R_A| - (sum of the rows of part, in row order).
+__global__ void __launch_bounds__(256)
+    esp_finish_kernel(const double* __restrict__ part, int rows, const double* __restrict__ atoms, int natom,
+                      const double* __restrict__ pts, int64_t n, double* __restrict__ out) {
+  const int64_t ip = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= n) return;
+  const double cx = pts[3 * ip], cy = pts[3 * ip + 1], cz = pts[3 * ip + 2];
+  double elec = 0.0;
+  for (int r = 0; r < rows; ++r) elec += part[(int64_t)r * n + ip];
   double nuc = 0.0;
   for (int a = 0; a < natom; ++a) {
     const double dx = cx - atoms[4 * a], dy = cy - atoms[4 * a + 1], dz = cz - atoms[4 * a + 2];
@@ -354,7 +385,8 @@ static int build_esp(ctc_molecule* mol) {
             hermite_e(A.l, B.l, a, b, ZAB, Ez);
             PairOut po;
             po.L = L;
-            po.pr = {(a * A.cx + b * B.cx) / p, (a * A.cy + b * B.cy) / p, (a * A.cz + b * B.cz) / p, p, pref};
+            po.pr = {(a * A.cx + b * B.cx) / p, (a * A.cy + b * B.cy) / p, (a * A.cz + b * B.cz) / p, p,
+                     0.5 * std::sqrt(kPi / p), 0.0};
             po.h.assign(NT, 0.0);
             const int LB1 = B.l + 1, L1 = L + 1;
             for (int ma = 0; ma < mA; ++ma) {
@@ -380,6 +412,7 @@ static int build_esp(ctc_molecule* mol) {
                   bnd += std::fabs(po.h[tuv_index(tt, uu, vv)]) * r_bound(p, tt + uu + vv);
             po.bound = bnd * pref;
             if (po.bound < eps) continue;
+            for (double& v : po.h) v *= pref;  // the kernels sum h_tuv R_tuv with 2 pi / p folded in
             outs[tid].push_back(std::move(po));
           }
         }
@@ -422,9 +455,10 @@ static int build_esp(ctc_molecule* mol) {
   std::vector<EspPair> pairs;
   std::vector<double> hv;
   std::vector<EspBatch> batches;
+  int lb0[kLmax + 2] = {};
   for (int L = 0; L <= kLmax; ++L) {
-    const int NT = ntuv(L);
-    const int per = std::max(1, std::min(kBatchPairs, kBatchH / NT));
+    const int per = batch_pairs(L);
+    lb0[L] = (int)batches.size();
     int in_batch = 0;
     for (auto& o : outs)
       for (auto& po : o) {
@@ -436,6 +470,7 @@ static int build_esp(ctc_molecule* mol) {
         if (++in_batch == per) in_batch = 0;
       }
   }
+  lb0[kLmax + 1] = (int)batches.size();
   if (hv.size() > (size_t)INT32_MAX) return fail(CTC_ERR_UNSUPPORTED, "ESP: too many pair coefficients");
   // Boys table
   std::vector<double> tab((size_t)kNT * kNF);
@@ -458,6 +493,7 @@ static int build_esp(ctc_molecule* mol) {
     e->mean_L += (double)np * bt.L;
   }
   if (!pairs.empty()) e->mean_L /= (double)pairs.size();
+  std::copy(lb0, lb0 + kLmax + 2, e->lb0);
   e->npairs = (int)pairs.size();
   e->nbatch = (int)batches.size();
   e->natom = mol->natom;
@@ -504,11 +540,55 @@ int eval_esp(ctc_molecule* mol, const double* d_points, int64_t n, double* d_out
     if (rc != CTC_OK) return rc;
   }
   const EspTables* e = mol->esp;
-  const int64_t grid = (n + kEspThreads - 1) / kEspThreads;
-  esp_kernel<<<(unsigned)grid, kEspThreads, 0, st>>>(e->d_pairs, e->d_h, e->d_batches, e->nbatch,
-                                                      e->d_boys, e->d_atoms, e->natom, d_points, n,
-                                                      d_out);
-  CTC_CUDA_TRY(cudaGetLastError());
+  int nsm = 148;
+  if (int rc = device_sm_count(&nsm); rc != CTC_OK) return rc;
+  // points per pass: bounds the partial-sum rows (rows x points x 8 B)
+  constexpr int64_t kChunk = (int64_t)1 << 22;
+  for (int64_t p0 = 0; p0 < n; p0 += kChunk) {
+    const int64_t m = std::min(kChunk, n - p0);
+    const int64_t gx = (m + kEspThreads - 1) / kEspThreads;
+    // slices of each class's batches: about 8 blocks per SM in every class kernel
+    int sl[kLmax + 1], rows = 0;
+    for (int L = 0; L <= kLmax; ++L) {
+      const int nb = e->lb0[L + 1] - e->lb0[L];
+      const int64_t want = (8 * (int64_t)nsm + gx - 1) / gx;
+      sl[L] = nb == 0 ? 0 : (int)std::max<int64_t>(1, std::min<int64_t>({want, (int64_t)nb, 65535}));
+      rows += sl[L];
+    }
+    if (int rc = mol->ws_esp.ensure(sizeof(double) * std::max<int64_t>(1, (int64_t)rows * m), st); rc != CTC_OK)
+      return rc;
+    double* part = (double*)mol->ws_esp.p;
+    const double* pts = d_points + 3 * p0;
+    int r = 0;
+    for (int L = 0; L <= kLmax; ++L) {
+      if (!sl[L]) continue;
+      const dim3 grid((unsigned)gx, (unsigned)sl[L]);
+      const int b0 = e->lb0[L], nb = e->lb0[L + 1] - e->lb0[L];
+      double* pr = part + (int64_t)r * m;
+#define CTC_ESP_CLASS(LL)                                                                                   \
+  case LL:                                                                                                  \
+    esp_class_kernel<LL><<<grid, kEspThreads, 0, st>>>(e->d_pairs, e->d_h, e->d_batches, b0, nb, e->d_boys, \
+                                                      pts, m, pr);                                         \
+    break;
+      switch (L) {
+        CTC_ESP_CLASS(0)
+        CTC_ESP_CLASS(1)
+        CTC_ESP_CLASS(2)
+        CTC_ESP_CLASS(3)
+        CTC_ESP_CLASS(4)
+        CTC_ESP_CLASS(5)
+        CTC_ESP_CLASS(6)
+        CTC_ESP_CLASS(7)
+        CTC_ESP_CLASS(8)
+      }
+#undef CTC_ESP_CLASS
+      CTC_CUDA_TRY(cudaGetLastError());
+      r += sl[L];
+    }
+    esp_finish_kernel<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(part, rows, e->d_atoms, e->natom, pts, m,
+                                                                   d_out + p0);
+    CTC_CUDA_TRY(cudaGetLastError());
+  }
   return CTC_OK;
 }
 
