@@ -87,8 +87,9 @@ double boys_series(int m, double T) {
 
 }  // namespace
 
-// pairs per batch of class L (a batch's Hermite coefficients fit 32 KB)
-constexpr int kBatchPairs = 64;
+// pairs per batch of class L: up to 256, with the batch's Hermite
+// coefficients within 32 KB (one barrier pair per batch in the class kernels)
+constexpr int kBatchPairs = 256;
 constexpr int kBatchH = 4096;
 __host__ __device__ constexpr int batch_pairs(int L) {
   return kBatchPairs < kBatchH / ntuv(L) ? kBatchPairs : kBatchH / ntuv(L);
@@ -224,6 +225,9 @@ __global__ void __launch_bounds__(kEspThreads)
     for (int i = threadIdx.x; i < np * NT; i += kEspThreads) sh[i] = hbuf[bt.h0 + i];
     __syncthreads();
     if (!live) continue;
+    // two pairs per iteration for the short classes: independent dependency
+    // chains for the FP64 pipe
+#pragma unroll(L <= 2 ? 2 : 1)
     for (int i = 0; i < np; ++i) {
       const EspPair q = sp[i];
       const double X = q.Px - cx, Y = q.Py - cy, Z = q.Pz - cz;
