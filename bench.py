@@ -207,12 +207,13 @@ def load_lib():
 
 
 def esp_roofline(lib, h, points, ms, fp64_peak):
-    """FP64-pipe roofline of the ESP kernel: algorithmic FP64 operations per point
-    (ctc_molecule_esp_info) x points / kernel time, against the measured FP64 peak."""
+    """FP64-pipe roofline of the ESP kernels (one per angular class, then the
+    fixed-order sum): algorithmic FP64 operations per point (ctc_molecule_esp_info)
+    x points / the call's device time, against the measured FP64 peak."""
     info = (C.c_double * 4)()
     check(lib, lib.ctc_molecule_esp_info(h, info), "esp_info")
     achieved = info[1] * points / (ms * 1e-3) / 1e12
-    return {"kernel": "esp_kernel (FP64 Boys + Hermite R recursion per primitive pair)", "bound": "fp64",
+    return {"kernel": "esp_class_kernel<L> per angular class + esp_finish_kernel (FP64 Boys + Hermite R recursion per primitive pair)", "bound": "fp64",
             "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s (fp64)", "frac": achieved / fp64_peak,
             "peak_source": "measured (cuBLAS DGEMM 8192^3, burst)",
             "flops_per_point": info[1], "primitive_pairs": info[0], "mean_L": info[3],

@@ -14,7 +14,7 @@
 // Screening.  An AO contributes only where its shell reaches: on the
 // 200-atom benchmark molecule ~9% of the AOs exceed 1e-14 at a typical grid
 // point.  Points are therefore grouped into spatially compact tiles (3-D
-// blocks of a cubic grid, or runs of Morton-sorted points), every tile builds
+// blocks of a cubic grid, or sort-tile-recursive runs of points), every tile builds
 // its own list of significant segments (distance from the tile's bounding
 // sphere below the segment's screening radius, where every AO value and
 // derivative has dropped below 1e-18), and the contraction of that tile runs

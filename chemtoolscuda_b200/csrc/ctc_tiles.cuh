@@ -2,7 +2,7 @@
 // descriptors (ctc_local.cu) and the adjoint (ctc_adjoint.cu).
 //
 // Points are grouped into spatially compact tiles (3-D blocks of a cubic grid,
-// or runs of Morton-sorted points); every tile lists the segments whose
+// or sort-tile-recursive runs of explicit points); every tile lists the segments whose
 // screening sphere (every AO value and derivative below 1e-18 outside it)
 // meets the tile's bounding sphere, and works on that compacted AO set only.
 // Per chunk of tiles: tile points -> screen -> AO block (compact) -> a
@@ -51,7 +51,8 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   return v;
 }
 
-// 30-bit Morton key of each point; a point with a non-finite coordinate gets
+// 30-bit Morton key of each point (the single-sort order of the fixed-scratch
+// entry point, ctc_noalloc.cu); a point with a non-finite coordinate gets
 // kNonFiniteKey, so the sort puts such points after every finite one and they
 // share tiles only with each other (and at most one tile's finite points).
 constexpr uint32_t kNonFiniteKey = 1u << 30;
@@ -71,6 +72,102 @@ __global__ void morton_kernel(const double* __restrict__ pts, int64_t n, double 
                 ? spread10(q(x, lox)) | (spread10(q(y, loy)) << 1) | (spread10(q(z, loz)) << 2)
                 : kNonFiniteKey;
   vals[i] = (int32_t)i;
+}
+
+// Sort-tile-recursive packing of explicit points (Leutenegger, Lopez and
+// Edgington, "STR: a simple and efficient algorithm for R-tree packing",
+// ICDE 1997): sort by x and cut into sx slabs of whole tiles; sort each slab
+// by y and cut it into sy columns; sort each column by z; tiles are then runs
+// of TP consecutive points.  sx and sy follow the points' bounding box
+// (edge a = (volume / P)^(1/3) for P tiles, sx ~ Lx / a, sy ~ Ly / a), so the
+// tiles are close to cubes also for slab-shaped point sets such as a
+// few-plane slice of a grid.  The box and the cut counts are formed on the
+// device (every thread of the key kernel derives the same counts), so the
+// host never waits.  Three radix sorts of 64-bit keys (group id << 32 |
+// coordinate key); a point with a non-finite coordinate gets the largest
+// coordinate key on every axis, so it sorts after every finite point and
+// shares tiles only with its kind (and at most one tile's finite points).
+__device__ __forceinline__ unsigned long long ordered_key(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ordered_value(unsigned long long k) {
+  return __longlong_as_double((long long)((k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k));
+}
+// box[0..2] = ordered keys of the minima, box[3..5] of the maxima (start at
+// all-ones and zero); finite points only
+__global__ void point_box_kernel(const double* __restrict__ pts, int64_t n, unsigned long long* box) {
+  unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0ull, 0ull, 0ull};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double* x = pts + 3 * i;
+    if (!finite_point(x)) continue;
+    for (int d = 0; d < 3; ++d) {
+      const unsigned long long k = ordered_key(x[d]);
+      mn[d] = k < mn[d] ? k : mn[d];
+      mx[d] = k > mx[d] ? k : mx[d];
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long a = __shfl_xor_sync(0xffffffffu, mn[d], o), b = __shfl_xor_sync(0xffffffffu, mx[d], o);
+      mn[d] = a < mn[d] ? a : mn[d];
+      mx[d] = b > mx[d] ? b : mx[d];
+    }
+  if ((threadIdx.x & 31) == 0)
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&box[d], mn[d]);
+      atomicMax(&box[3 + d], mx[d]);
+    }
+}
+struct StrShape {
+  double lo[3], scale[3];  // coordinate key = (x - lo) * scale, clamped
+  int64_t Sx, Scol, c;     // points per slab, points per column, columns per slab
+};
+__device__ StrShape str_shape(const unsigned long long* __restrict__ box, int64_t P, int TP) {
+  StrShape sh;
+  double L[3];
+  bool any = box[0] <= box[3];
+  double Lmax = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    sh.lo[d] = any ? ordered_value(box[d]) : 0.0;
+    L[d] = any ? ordered_value(box[3 + d]) - sh.lo[d] : 0.0;
+    Lmax = fmax(Lmax, L[d]);
+  }
+  if (!(Lmax > 0.0)) Lmax = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    L[d] = fmax(L[d], 1e-3 * Lmax);  // planar or linear sets: keep the volume positive
+    sh.scale[d] = 4294967040.0 / L[d];
+  }
+  const double a = cbrt(L[0] * L[1] * L[2] / (double)P);
+  int64_t sx = (int64_t)fmin(fmax(rint(L[0] / a), 1.0), (double)P);
+  const int64_t Tsl = (P + sx - 1) / sx;
+  int64_t sy = (int64_t)fmin(fmax(rint(L[1] / a), 1.0), (double)Tsl);
+  const int64_t Tcol = (Tsl + sy - 1) / sy;
+  sy = (Tsl + Tcol - 1) / Tcol;
+  sh.Sx = Tsl * TP;
+  sh.Scol = Tcol * TP;
+  sh.c = sy;
+  return sh;
+}
+__device__ __forceinline__ uint32_t axis_key(double v, double lo, double scale) {
+  double c = (v - lo) * scale;
+  c = c < 0.0 ? 0.0 : (c > 4294967040.0 ? 4294967040.0 : c);
+  return (uint32_t)c;
+}
+__global__ void str_key_kernel(const double* __restrict__ pts, const int32_t* __restrict__ perm,
+                               int64_t n, int pass, const unsigned long long* __restrict__ box,
+                               int64_t P, int TP, uint64_t* __restrict__ keys, int32_t* __restrict__ vals) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const StrShape sh = str_shape(box, P, TP);
+  const int64_t p = perm ? perm[i] : i;
+  const double* x = pts + 3 * p;
+  uint64_t g = 0;
+  if (pass == 1) g = (uint64_t)(i / sh.Sx);
+  if (pass == 2) g = (uint64_t)(i / sh.Sx) * (uint64_t)sh.c + (uint64_t)((i % sh.Sx) / sh.Scol);
+  const uint32_t k = finite_point(x) ? axis_key(x[pass], sh.lo[pass], sh.scale[pass]) : 0xFFFFFFFFu;
+  keys[i] = (g << 32) | k;
+  vals[i] = (int32_t)p;
 }
 
 // Tiles of TP consecutive sorted points; padding slots repeat the tile's first point.
@@ -608,41 +705,35 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     ntiles = (n + TP - 1) / TP;
   }
   int rc;
-  // explicit points: Morton order over the molecule's box padded by 12 bohr
+  // explicit points: sort-tile-recursive order over the points' own box
   int32_t* perm = nullptr;
   if (!src.cubic) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int a = 0; a < mol->natom; ++a)
-      for (int d = 0; d < 3; ++d) {
-        lo[d] = std::min(lo[d], mol->atom_xyz[3 * a + d]);
-        hi[d] = std::max(hi[d], mol->atom_xyz[3 * a + d]);
-      }
-    if (mol->natom == 0)
-      for (int d = 0; d < 3; ++d) { lo[d] = -1; hi[d] = 1; }
-    double ext = 0;
-    for (int d = 0; d < 3; ++d) {
-      lo[d] -= 12.0;
-      hi[d] += 12.0;
-      ext = std::max(ext, hi[d] - lo[d]);
-    }
     size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0,
-                                    kMortonSortBits, st);
-    const size_t need = 4 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 64, st);
+    const size_t need = 2 * sizeof(uint64_t) * (size_t)n + 2 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
     if ((rc = mol->ws_part.ensure(need, st)) != CTC_OK) return rc;
     Carve cv{(char*)mol->ws_part.p};
-    uint32_t* k_in = cv.take<uint32_t>(n);
-    uint32_t* k_out = cv.take<uint32_t>(n);
+    unsigned long long* box = cv.take<unsigned long long>(6);
+    uint64_t* k_in = cv.take<uint64_t>(n);
+    uint64_t* k_out = cv.take<uint64_t>(n);
     int32_t* v_in = cv.take<int32_t>(n);
     perm = cv.take<int32_t>(n);
     void* tmp = cv.take<char>(tmp_bytes);
-    morton_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src.pts, n, lo[0], lo[1], lo[2],
-                                                                1024.0 / ext, k_in, v_in);
+    CTC_CUDA_TRY(cudaMemsetAsync(box, 0xFF, 3 * sizeof(unsigned long long), st));
+    CTC_CUDA_TRY(cudaMemsetAsync(box + 3, 0, 3 * sizeof(unsigned long long), st));
+    point_box_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * 148), 256, 0, st>>>(src.pts, n, box);
     CTC_CUDA_TRY(cudaGetLastError());
-    CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
-                                                 kMortonSortBits, st));
-    mol->host_launches += 2;
+    // group ids of passes 2 and 3 are below sx * sy <= sx * ceil(P / sx) < P + sx <= 2 P
+    const int gbits = 64 - __builtin_clzll((unsigned long long)(2 * ntiles));
+    const unsigned g = (unsigned)((n + 255) / 256);
+    for (int pass = 0; pass < 3; ++pass) {
+      str_key_kernel<<<g, 256, 0, st>>>(src.pts, pass ? perm : nullptr, n, pass, box, ntiles, TP, k_in, v_in);
+      CTC_CUDA_TRY(cudaGetLastError());
+      CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
+                                                   32 + (pass ? gbits : 0), st));
+    }
+    mol->host_launches += 7;
   }
   // tile points of tiles [t0, t0 + tb.C)
   auto tile_points = [&](const TileBatch& tb, int64_t t0) -> int {
