@@ -473,6 +473,7 @@ int ctc_molecule_destroy(ctc_molecule* m) {
   m->ws_misc.release();
   m->ws_cap.release();
   m->ws_esp.release();
+  m->ws_adj.release();
   if (m->hostpipe) {
     m->hostpipe->release();
     delete m->hostpipe;

@@ -180,7 +180,7 @@ struct ctc_molecule {
   bool prof = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_ev[2];
   // scratch
-  ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc, ws_cap, ws_esp;
+  ctc::Scratch ws_ao, ws_sl, ws_part, ws_misc, ws_cap, ws_esp, ws_adj;
   ctc::EspTables* esp = nullptr;
   bool esp_valid = false;
   ctc::HostPipe* hostpipe = nullptr;
