@@ -873,9 +873,56 @@ def run_workload(args):
                      "roofline": roof,
                      "parity": {"sample_points": 64, "max_rel_err": rel, "tolerance": 1e-8}})
         lib.ctc_molecule_destroy(h)
+    elif w == "c4adj":
+        line.update(_c4_adjoint_subcube(args))
     else:
         raise SystemExit(f"unknown workload {w}")
     return line
+
+
+def _c4_adjoint_subcube(args):
+    """Forward (rho, grad rho, FP64) and backward (dL/dD) of the GGA functional
+    on a central sub-cube (--shape, default 64^3 here) of the c4 molecule's 368^3
+    cube at 0.25 bohr: the densest part of the molecule, where a 128-point tile
+    keeps ~2 800 functions.  Forward and backward timed separately with CUDA
+    events; a small case for profiling the adjoint kernel."""
+    import torch
+    from chemtoolscuda_b200 import molecule_from_synthetic
+    from chemtoolscuda_b200.autograd import density_and_gradient, gga_functional
+    mol = S.make_molecule("c4", seed=0)
+    shape = tuple(args.shape) if tuple(args.shape) != tuple(SHAPE) else (64, 64, 64)
+    origin, axes = S.cube_grid(mol, 0.25, (368, 368, 368))
+    off = [(368 - s_) // 2 for s_ in shape]
+    so = np.asarray(origin) + np.asarray(off) @ np.asarray(axes)
+    pm = molecule_from_synthetic(mol)
+    R = torch.as_tensor(mol.coords)
+    pts = torch.as_tensor(S.cube_points(so, axes, shape), device="cuda")
+    wts = torch.full((pts.shape[0],), 0.25 ** 3, dtype=torch.float64, device="cuda")
+    D = torch.as_tensor(mol.D, device="cuda").requires_grad_(True)
+    fw, bw = [], []
+    for it in range(args.warmup + args.steps):
+        D.grad = None
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        rho, grad = density_and_gradient(pm, pts, D, R)
+        Lv = gga_functional(rho, grad, wts)
+        e[1].record()
+        Lv.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            fw.append(e[0].elapsed_time(e[1]))
+            bw.append(e[1].elapsed_time(e[2]))
+    n = int(pts.shape[0])
+    ms = statistics.mean(fw) + statistics.mean(bw)
+    return {"metric": "grid pts/s for forward (rho, grad rho) + adjoint dL/dD of a GGA functional, "
+                      "1000-atom molecule, central sub-cube",
+            "value": n / (ms * 1e-3), "unit": "grid points/s", "ms_per_step": ms,
+            "forward_ms": statistics.mean(fw), "backward_ms": statistics.mean(bw),
+            "higher_is_better": True, "dtype": "f64",
+            "config": {"workload": f"c4 adjoint: 1000 atoms (Cartesian up to g), central {shape[0]}x{shape[1]}x{shape[2]} "
+                                   "sub-cube of the 368^3 cube at 0.25 bohr",
+                       "nbasis": mol.nbasis, "points": n}}
 
 
 def _c4_adjoint(mol, origin, axes, shape, args):
@@ -960,7 +1007,7 @@ def main():
                     help="reference arm: surface points of its ESP sample")
     ap.add_argument("--ref-points", type=int, default=0,
                     help="reference arm points per step (0: the largest batch its 32-bit indexing allows)")
-    ap.add_argument("--workload", default=None, choices=["c1", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default=None, choices=["c1", "c3", "c4", "c4adj", "c5"],
                     help="measure another configuration instead of the headline one (one GPU)")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
