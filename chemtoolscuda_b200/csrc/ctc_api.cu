@@ -42,25 +42,46 @@ double** slot(ctc_outputs* o, int i) {
   return s[i];
 }
 
-// memcpy of large host buffers on several threads: one thread moves ~5-10
+// memcpy of large host buffers on several threads: one thread moves ~4-10
 // GB/s, and the host side of the host-buffer pipeline moves ~160 B per point.
-void par_copy(void* dst, const void* src, size_t bytes) {
-  constexpr size_t kSlice = (size_t)8 << 20;
+// One copy job -- a list of (dst, src, bytes) segments, e.g. all outputs of a
+// slab -- is cut at equal byte offsets over up to 16 threads, so small and
+// large outputs share the threads (one output at a time left the 8 MB
+// outputs of a 2^20-point slab on one thread each).
+struct CopySeg {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+void par_copy_segs(const std::vector<CopySeg>& segs) {
+  size_t total = 0;
+  for (const CopySeg& g : segs) total += g.bytes;
+  constexpr size_t kSlice = (size_t)2 << 20;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nt = std::min<size_t>({(size_t)8, (size_t)hw, (bytes + kSlice - 1) / kSlice});
+  const size_t nt = std::max<size_t>(1, std::min<size_t>({(size_t)16, (size_t)hw, total / kSlice}));
+  auto run = [&](size_t lo, size_t hi) {  // bytes [lo, hi) of the concatenated segments
+    size_t base = 0;
+    for (const CopySeg& g : segs) {
+      const size_t a = std::max(lo, base), b = std::min(hi, base + g.bytes);
+      if (a < b) std::memcpy((char*)g.dst + (a - base), (const char*)g.src + (a - base), b - a);
+      base += g.bytes;
+    }
+  };
   if (nt <= 1) {
-    std::memcpy(dst, src, bytes);
+    run(0, total);
     return;
   }
+  const size_t part = (total + nt - 1) / nt;
   std::vector<std::thread> th;
-  const size_t part = (bytes + nt - 1) / nt;
   for (size_t t = 1; t < nt; ++t) {
-    const size_t b0 = t * part, b1 = std::min(bytes, b0 + part);
-    if (b0 < b1) th.emplace_back([=] { std::memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0); });
+    const size_t lo = t * part, hi = std::min(total, lo + part);
+    if (lo < hi) th.emplace_back(run, lo, hi);
   }
-  std::memcpy(dst, src, std::min(bytes, part));
+  run(0, std::min(total, part));
   for (auto& x : th) x.join();
 }
+
+void par_copy(void* dst, const void* src, size_t bytes) { par_copy_segs({{dst, src, bytes}}); }
 
 }  // namespace
 
@@ -213,12 +234,14 @@ int ctc_eval_local_host(ctc_molecule* mol, const double* h_points, int64_t n, in
     if (pending_off[b] < 0 || rc != CTC_OK) return;
     if (!cuda_ok(cudaEventSynchronize(hp.ev_out[b]), "ctc_eval_local_host: wait")) return;
     const double* hb = (const double*)hp.pin[b] + 3 * (size_t)pending_n[b];
+    std::vector<CopySeg> segs;
     for (int i = 0; i < 12; ++i) {
       double* dst = *slot(const_cast<ctc_outputs*>(h_out), i);
       if (!dst) continue;
-      par_copy(dst + kWidth[i] * pending_off[b], hb, sizeof(double) * kWidth[i] * pending_n[b]);
+      segs.push_back({dst + kWidth[i] * pending_off[b], hb, sizeof(double) * kWidth[i] * pending_n[b]});
       hb += kWidth[i] * pending_n[b];
     }
+    par_copy_segs(segs);
     pending_off[b] = -1;
   };
   int b = 0;

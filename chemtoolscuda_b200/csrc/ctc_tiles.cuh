@@ -690,6 +690,7 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
                      cudaStream_t st, const std::function<int(const TileBatch&)>& compute,
                      const std::function<int(const TileBatch&)>* ao_launch = nullptr,
                      int rows = 128) {
+  if (n <= 0) return CTC_OK;  // (no zero-sized grids below)
   // cubic-grid tiles: blocks of 2x4x4 or 4x4x8 grid points
   int TX = 2, TY = 4, TZ = 4;
   if (TP == 128) { TX = 4; TY = 4; TZ = 8; }
