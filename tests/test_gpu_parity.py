@@ -157,6 +157,46 @@ def test_edge_cases(torch_cuda):
     assert_close("ragged hess", got["hess"], ref["hess"], sc["hess"], 1e-10, 1e-14)
 
 
+@pytest.mark.parametrize("precision,rtol", [(ctc_abi.PREC_FP64, 1e-10), (ctc_abi.PREC_TC, 1e-8)])
+def test_degenerate_point_sets(torch_cuda, precision, rtol):
+    """Explicit points are packed into tiles by their bounding box (sort by x,
+    y, z with cut counts from the box); a set with no extent along one or two
+    axes, repeated points, and finite points mixed with non-finite ones must
+    give the same outputs as the oracle."""
+    mol, pts = _cases().CASES["c1"]()
+    m = _mol(mol)
+    rng = np.random.default_rng(11)
+    c = mol.coords.mean(0)
+    u = rng.uniform(-3, 3, size=(700, 2))
+    sets = {
+        "plane": np.column_stack([c[0] + u[:, 0], c[1] + u[:, 1], np.full(700, c[2] + 0.3)]),
+        "line": np.column_stack([np.full(500, c[0] - 0.2), np.full(500, c[1] + 0.1),
+                                 c[2] + np.linspace(-4, 4, 500)]),
+        "repeated": np.repeat(pts[:3], 50, axis=0),
+        "single": pts[:1],
+    }
+    keys = ("rho", "grad", "hess", "lap")
+    for name, p in sets.items():
+        got = m.eval_local(p, keys, precision=precision)
+        ref = O.eval_local(mol.flat(), mol.D, p, keys=keys)
+        sc = term_scales(mol.flat(), mol.D, p)
+        for k in keys:
+            assert_close(f"{name} {k}", got[k], ref[k], sc[k], rtol, 1e-14)
+    # finite points interleaved with non-finite ones: NaN outputs only where the point is
+    p = S.random_points(rng, mol, 300)
+    bad = rng.choice(300, 40, replace=False)
+    p[bad[:20], 0] = np.nan
+    p[bad[20:], 2] = np.inf
+    got = m.eval_local(p, ("rho", "grad"), precision=precision)
+    ok = np.ones(300, bool)
+    ok[bad] = False
+    assert np.isnan(got["rho"][~ok]).all()
+    ref = O.eval_local(mol.flat(), mol.D, p[ok], keys=("rho", "grad"))
+    sc = term_scales(mol.flat(), mol.D, p[ok])
+    assert_close("mixed rho", got["rho"][ok], ref["rho"], sc["rho"], rtol, 1e-14)
+    assert_close("mixed grad", got["grad"][ok], ref["grad"], sc["grad"], rtol, 1e-14)
+
+
 def test_invalid_basis_rejected(torch_cuda):
     mol, _ = _cases().CASES["c1"]()
     f = mol.flat()
