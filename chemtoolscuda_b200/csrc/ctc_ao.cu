@@ -209,7 +209,7 @@ __device__ __forceinline__ void eval_dispatch(const DevSeg& sg, const double* __
 //
 // SLICE = 4 or 1 also produces the row exponents of the tensor-core split
 // operands of the tile (ctc_split.cuh): the rows are the tile's points x {phi,
-// d_x, d_y, d_z phi} (SLICE = 4, blocks of 32 points x 4 quantities, TP <= 64)
+// d_x, d_y, d_z phi} (SLICE = 4, blocks of 32 points x 4 quantities, TP = 32)
 // or its points x phi (SLICE = 1, TP <= 256).  Every lane keeps the running
 // maximum of its values while it evaluates, so the exponents cost no second
 // pass over the block; slice_rows_kernel then writes the digit planes.
@@ -356,7 +356,7 @@ int launch_ao_tiles(const ctc_molecule* mol, const TileBatch& tb, int deriv, cud
 int launch_ao_tiles_sliced(const ctc_molecule* mol, const TileBatch& tb, int deriv, int nqa,
                            int8_t* planes, int32_t* eexp, const int32_t* order, cudaStream_t st) {
   if (tb.C <= 0) return CTC_OK;
-  if (!(nqa == 4 && (tb.TP == 32 || tb.TP == 64) && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
+  if (!(nqa == 4 && tb.TP == 32 && deriv >= 1) && !(nqa == 1 && tb.TP == 128))
     return fail(CTC_ERR_INVALID, "sliced AO tiles: unsupported row layout");
   if (planes == nullptr || eexp == nullptr)
     return fail(CTC_ERR_INVALID, "sliced AO tiles: null workspace");
