@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(kEspThreads)
                      const double* __restrict__ pts, int64_t n, double* __restrict__ part) {
   constexpr int NT = ntuv(L);
   constexpr int BP = batch_pairs(L);
+  constexpr bool PAIRS2 = L <= 4;  // registers stay below ~170 up to L = 4
   __shared__ EspPair sp[BP];
   __shared__ double sh[BP * NT];
   const int slices = gridDim.y, y = blockIdx.y;
@@ -225,10 +226,7 @@ __global__ void __launch_bounds__(kEspThreads)
     for (int i = threadIdx.x; i < np * NT; i += kEspThreads) sh[i] = hbuf[bt.h0 + i];
     __syncthreads();
     if (!live) continue;
-    // two pairs per iteration for the short classes: independent dependency
-    // chains for the FP64 pipe
-#pragma unroll(L <= 2 ? 2 : 1)
-    for (int i = 0; i < np; ++i) {
+    auto pair_sum = [&](int i) -> double {
       const EspPair q = sp[i];
       const double X = q.Px - cx, Y = q.Py - cy, Z = q.Pz - cz;
       double G[L + 1];
@@ -239,8 +237,19 @@ __global__ void __launch_bounds__(kEspThreads)
       double s = 0.0;
 #pragma unroll
       for (int k = 0; k < NT; ++k) s += h[k] * R[k];
-      acc += s;
+      return s;
+    };
+    int i = 0;
+    if (PAIRS2) {
+      // two pairs per iteration: two independent dependency chains (Boys, R
+      // recursion, dot product) for the FP64 pipe; added in pair order
+      for (; i + 1 < np; i += 2) {
+        const double s0 = pair_sum(i), s1 = pair_sum(i + 1);
+        acc += s0;
+        acc += s1;
+      }
     }
+    for (; i < np; ++i) acc += pair_sum(i);
   }
   if (live) part[(int64_t)y * n + ip] = acc;
 }
