@@ -25,10 +25,14 @@
 // operands of each K block (one thread issues the TMA loads of the five A
 // planes; all 128 threads gather the five D planes by compact index from the
 // packed copy of D and write them in the 64-byte-swizzled K-major layout),
-// warp 4 issues the MMAs from one thread and commits them to mbarriers, warps
-// 5-8 drain the TMEM accumulators (one 32-lane quarter each) into an FP64 copy
-// of G in shared memory and run the epilogue while the next nu tile's MMAs
-// run.  Every mbarrier wait is bounded: on timeout the kernel records a
+// warps 4-7 drain the TMEM accumulators (one 32-lane quarter each) into an
+// FP64 copy of G in shared memory and run the epilogue while the next nu
+// tile's MMAs run, warp 8 issues the MMAs from one thread and commits them to
+// mbarriers.  Registers move from the producer warpgroup (104 each) to the
+// epilogue warpgroup (232 each), whose AO loads in flight are bounded by
+// registers (setmaxnreg; 128 x 104 + 128 x 232 + 32 x 168 = the 288 x 168 of
+// the launch, and per SM sub-partition 104 + 232 + 168 registers x 32 lanes
+// stay within 16 384).  Every mbarrier wait is bounded: on timeout the kernel records a
 // status code, stops issuing work, and the allocating warp still frees its
 // TMEM.
 #include <cuda.h>
@@ -66,6 +70,11 @@ constexpr int kBStageBytes = kPlanes * kBPlaneBytes;
 constexpr int kGBytes = kN * kRows * 8;         // FP64 copy of one nu tile of G (64 KB)
 constexpr int kSmemTc = kStages * (kAStageBytes + kBStageBytes) + kGBytes + 1024;  // + alignment slack
 constexpr int kThreadsTc = 288;
+constexpr int kMmaWarp = 8;             // warps 0-3 producers, 4-7 epilogue, 8 MMA
+constexpr int kProducerRegs = 104;      // setmaxnreg shares (launch: 168 each)
+constexpr int kEpilogueRegs = 232;
+static_assert(4 * 32 * kProducerRegs + 4 * 32 * kEpilogueRegs + 32 * 168 <= kThreadsTc * 168,
+              "register split above the launch's total");
 constexpr int kMaxKt = 16384;
 constexpr uint32_t kStatusTimeout = 0x7101;
 // readers of a tile-ring slot: 4 producer warps, the MMA warp, one epilogue thread
@@ -255,12 +264,14 @@ __device__ __forceinline__ constexpr int role_sum(int role, int slot, int row) {
 // the role's i-th sum (slot-major, rows in order).  G is the FP64 copy in
 // shared memory, [column][row]; ao points at AO quantity 0, column 0 of the nu
 // tile for this thread's point (element (q, c) at ao[q * ldq + c * 32]).
-// AO columns per load group of the epilogue contraction: 16 / GW register
-// buffers keep 16 - GW columns of AO values in flight per thread while one
-// group is reduced (measured on the 215^3 cube: GW = 2 beats 8 (335 -> 317 ms),
-// 4 (328 ms) and 1 (318 ms); the loads are latency-bound on tiles with few
-// columns)
+// AO columns per load group of the epilogue contraction: kEpiColumns / GW
+// register buffers keep kEpiColumns - GW columns of AO values in flight per
+// thread while one group is reduced (measured on the 215^3 cube with 16
+// columns: GW = 2 beat 8 (335 -> 317 ms), 4 (328 ms) and 1 (318 ms); the loads
+// are latency-bound on tiles with few columns, so the epilogue warpgroup takes
+// the producers' spare registers for 28)
 constexpr int kEpiGroup = 2;
+constexpr int kEpiColumns = 28;
 
 template <int ROLE, int GW>
 __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int64_t ldq,
@@ -268,7 +279,7 @@ __device__ __forceinline__ void contract_role(const double* __restrict__ ao, int
                                               uint64_t stream, double* acc) {
   constexpr int NS = role_nslot(ROLE);
   constexpr int NG = kN / GW;    // groups of GW columns
-  constexpr int NB = 16 / GW;    // register buffers of one group each
+  constexpr int NB = kEpiColumns / GW;  // register buffers of one group each
   bool live[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) live[s] = role_q(ROLE, s) < nq_ao;
@@ -491,7 +502,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (warp == 4) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(
                      smem_u32(&tmem_base_sh)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
@@ -537,6 +548,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
 
   if (warp < 4) {
     // ---------------- producers
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kProducerRegs));
     // Thread tid owns the 4 mu columns k4 = (tid % 16) * 4 of every stage and the
     // 8 nu rows n = tid / 16 + 8 i of every nu tile; its 32 gathers of D are
     // independent.  Stages are software-pipelined one ahead: the AO indices of
@@ -661,7 +673,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       args.trace[(int64_t)blockIdx.x * 8 + 1] = tr0;
       args.trace[(int64_t)blockIdx.x * 8 + 2] = clock64() - t_start - tr0;
     }
-  } else if (warp == 4) {
+  } else if (warp == kMmaWarp) {
     // ---------------- MMA issuer
     // One MMA per A digit plane pa and K step: B is the stage's first D planes
     // read as one operand of 64 * nb rows (the planes are contiguous), so the
@@ -741,7 +753,8 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
       args.trace[(int64_t)blockIdx.x * 8 + 4] = tr1;
     }
   } else {
-    // ---------------- epilogue (warps 5..8 -> TMEM lane quarters 1,2,3,0)
+    // ---------------- epilogue (warps 4..7 -> TMEM lane quarters 0..3)
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kEpilogueRegs));
     // Per nu tile: drain the five level accumulators of this warp's TMEM lane
     // quarter into one FP64 value per element, scaled, in the shared-memory
     // copy of G; release TMEM (the MMA warp starts the next nu tile); then
@@ -749,7 +762,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
     // final sums are formed while the MMAs of the next tile run.
     const int quarter = warp & 3;
     const int r = quarter * 32 + lane;        // TMEM lane / G row drained by this thread
-    const int role = warp - 5;                // 0..3
+    const int role = warp - 4;                // 0..3
     const int etid = role * 32 + lane;        // 0..127
     constexpr int PTS = kRows / NQA;
     const int nq_ao = tb.nq;
@@ -882,7 +895,7 @@ __global__ void __launch_bounds__(kThreadsTc, 1)
   __syncthreads();
   if (args.trace && threadIdx.x == 0) args.trace[(int64_t)blockIdx.x * 8] = clock64() - t_start;
   if (s_abort && threadIdx.x == 0) atomicExch(args.status, (int32_t)kStatusTimeout);
-  if (warp == 4) {
+  if (warp == kMmaWarp) {
     // every MMA this thread issued has completed before TMEM is released
     if (lane == 0) umma_commit(&done_bar);
     __syncwarp();
