@@ -649,6 +649,51 @@ def run_reference(args, ws, rank):
             "esp": esp}
 
 
+def run_reference_c1(args):
+    """The reference's own density driver on the c1 workload: the 12-atom
+    molecule (Cartesian up to d) and the same 1e5 seeded points as this build's
+    c1 line, rho only, timed by wall clock around its synchronous host API."""
+    libp = os.path.join(ROOT, "oracle", "_ref", "libctc_ref.so")
+    if not os.path.exists(libp):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libctc_ref.so not built (make -C oracle ref)"}
+    lib = C.CDLL(libp)
+    vp, i32 = C.c_void_p, C.c_int
+    lib.ref_create.restype = vp
+    lib.ref_create.argtypes = [i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, i32]
+    lib.ref_last_error.restype = C.c_char_p
+    lib.ref_density.argtypes = [vp, vp, i32, vp]
+    mol = S.make_molecule("c1", seed=0)
+    pts = np.ascontiguousarray(S.random_points(np.random.default_rng(1), mol, 100000, pad=4.0))
+    n = len(pts)
+    f = mol.flat()
+    keep = [np.ascontiguousarray(f[k]) for k in ("centers", "nprim", "nseg", "angmoms", "exps", "coeffs")]
+    xyz, chg, D = np.ascontiguousarray(mol.coords), np.ascontiguousarray(mol.charges), np.ascontiguousarray(mol.D)
+    h = lib.ref_create(len(f["nprim"]), *[k.ctypes.data for k in keep], len(xyz), xyz.ctypes.data,
+                       chg.ctypes.data, D.ctypes.data, D.shape[0])
+    if not h:
+        return {"impl": "reference", "unavailable": lib.ref_last_error().decode()}
+    out = np.empty(n)
+
+    def step():
+        if lib.ref_density(h, pts.ctypes.data, n, out.ctypes.data) != 0:
+            raise RuntimeError(lib.ref_last_error().decode())
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    value = n * args.steps / el
+    return {"impl": "reference", "workload_id": "c1", "n_gpus": 1, "data": "synthetic",
+            "metric": "grid pts/s for rho (12-atom molecule, 1e5 points)", "value": value,
+            "unit": "grid points/s", "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "dtype": "f64", "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": "c1: 12 atoms, Cartesian up to d, 1e5 uniform points, rho only",
+                       "nbasis": mol.nbasis, "points": n},
+            "timing": "wall clock around evaluate_electron_density_on_any_grid (host arrays in and out)",
+            "e2e": {"value": value, "unit": "grid points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 # --------------------------------------------------------------------------- main
 # --------------------------------------------------------------------------- other configurations
 PARITY_ATOL = 1e-14
@@ -1013,7 +1058,16 @@ def main():
     ws, rank, local = dist_setup()
     if args.workload is not None:
         if rank == 0:
-            print(json.dumps(run_workload(args)), flush=True)
+            if args.impl == "reference":
+                line = (run_reference_c1(args) if args.workload == "c1" else
+                        {"impl": "reference", "workload_id": args.workload,
+                         "unavailable": "this build's reference arm covers the headline configuration "
+                                        "(with its ESP on the 90-atom sub-molecule) and c1 only; the "
+                                        "reference has no adjoint driver (c3, c4adj) and no ESP for the "
+                                        "100-atom c5 basis (constant-memory cap)"})
+            else:
+                line = run_workload(args)
+            print(json.dumps(line), flush=True)
         if ws > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
