@@ -51,8 +51,9 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   return v;
 }
 
-// 30-bit Morton key of each point (the single-sort order of the fixed-scratch
-// entry point, ctc_noalloc.cu); a point with a non-finite coordinate gets
+// 30-bit Morton key of each point (the single-sort order of small calls and
+// of the fixed-scratch entry point, ctc_noalloc.cu); a point with a
+// non-finite coordinate gets
 // kNonFiniteKey, so the sort puts such points after every finite one and they
 // share tiles only with each other (and at most one tile's finite points).
 constexpr uint32_t kNonFiniteKey = 1u << 30;
@@ -706,12 +707,21 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     ntiles = (n + TP - 1) / TP;
   }
   int rc;
-  // explicit points: sort-tile-recursive order over the points' own box
+  // explicit points: sort-tile-recursive order over the points' own box for
+  // calls of kStrMinPoints points or more; below that, one sort of 30-bit
+  // Morton keys over the molecule's box padded by 12 bohr (three sorts cost
+  // ~0.4 ms, as much as a whole 1e5-point density call of a small molecule,
+  // while the tiles' shape matters little there)
+  constexpr int64_t kStrMinPoints = (int64_t)1 << 18;
   int32_t* perm = nullptr;
   if (!src.cubic) {
-    size_t tmp_bytes = 0;
+    const bool str = n >= kStrMinPoints;
+    size_t tmp_bytes = 0, tmp32 = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
                                     (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, 64, st);
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp32, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (int32_t*)nullptr, (int32_t*)nullptr, (int)n, 0, kMortonSortBits, st);
+    tmp_bytes = std::max(tmp_bytes, tmp32);
     const size_t need = 2 * sizeof(uint64_t) * (size_t)n + 2 * sizeof(int32_t) * (size_t)n + tmp_bytes + 4096;
     if ((rc = mol->ws_part.ensure(need, st)) != CTC_OK) return rc;
     Carve cv{(char*)mol->ws_part.p};
@@ -721,20 +731,41 @@ inline int run_tiles(ctc_molecule* mol, const PointSrc& src, int64_t n, int TP, 
     int32_t* v_in = cv.take<int32_t>(n);
     perm = cv.take<int32_t>(n);
     void* tmp = cv.take<char>(tmp_bytes);
-    CTC_CUDA_TRY(cudaMemsetAsync(box, 0xFF, 3 * sizeof(unsigned long long), st));
-    CTC_CUDA_TRY(cudaMemsetAsync(box + 3, 0, 3 * sizeof(unsigned long long), st));
-    point_box_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * 148), 256, 0, st>>>(src.pts, n, box);
-    CTC_CUDA_TRY(cudaGetLastError());
-    // group ids of passes 2 and 3 are below sx * sy <= sx * ceil(P / sx) < P + sx <= 2 P
-    const int gbits = 64 - __builtin_clzll((unsigned long long)(2 * ntiles));
-    const unsigned g = (unsigned)((n + 255) / 256);
-    for (int pass = 0; pass < 3; ++pass) {
-      str_key_kernel<<<g, 256, 0, st>>>(src.pts, pass ? perm : nullptr, n, pass, box, ntiles, TP, k_in, v_in);
+    if (str) {
+      CTC_CUDA_TRY(cudaMemsetAsync(box, 0xFF, 3 * sizeof(unsigned long long), st));
+      CTC_CUDA_TRY(cudaMemsetAsync(box + 3, 0, 3 * sizeof(unsigned long long), st));
+      point_box_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * 148), 256, 0, st>>>(src.pts, n, box);
       CTC_CUDA_TRY(cudaGetLastError());
-      CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
-                                                   32 + (pass ? gbits : 0), st));
+      // group ids of passes 2 and 3 are below sx * sy <= sx * ceil(P / sx) < P + sx <= 2 P
+      const int gbits = 64 - __builtin_clzll((unsigned long long)(2 * ntiles));
+      const unsigned g = (unsigned)((n + 255) / 256);
+      for (int pass = 0; pass < 3; ++pass) {
+        str_key_kernel<<<g, 256, 0, st>>>(src.pts, pass ? perm : nullptr, n, pass, box, ntiles, TP, k_in, v_in);
+        CTC_CUDA_TRY(cudaGetLastError());
+        CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k_in, k_out, v_in, perm, (int)n, 0,
+                                                     32 + (pass ? gbits : 0), st));
+      }
+      mol->host_launches += 7;
+    } else {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int a = 0; a < mol->natom; ++a)
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min(lo[d], mol->atom_xyz[3 * a + d]);
+          hi[d] = std::max(hi[d], mol->atom_xyz[3 * a + d]);
+        }
+      if (mol->natom == 0)
+        for (int d = 0; d < 3; ++d) { lo[d] = -1; hi[d] = 1; }
+      double ext = 0;
+      for (int d = 0; d < 3; ++d) ext = std::max(ext, hi[d] - lo[d] + 24.0);
+      uint32_t* k32_in = (uint32_t*)k_in;
+      uint32_t* k32_out = (uint32_t*)k_out;
+      morton_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src.pts, n, lo[0] - 12.0, lo[1] - 12.0,
+                                                                  lo[2] - 12.0, 1024.0 / ext, k32_in, v_in);
+      CTC_CUDA_TRY(cudaGetLastError());
+      CTC_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k32_in, k32_out, v_in, perm, (int)n, 0,
+                                                   kMortonSortBits, st));
+      mol->host_launches += 2;
     }
-    mol->host_launches += 7;
   }
   // tile points of tiles [t0, t0 + tb.C)
   auto tile_points = [&](const TileBatch& tb, int64_t t0) -> int {

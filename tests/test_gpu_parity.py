@@ -117,6 +117,31 @@ def test_cubic_grid_matches_points(torch_cuda):
     assert_close("cubic grad", got["grad"].reshape(-1, 3), ref["grad"], sc["grad"], 1e-10, 1e-14)
 
 
+@pytest.mark.parametrize("precision,rtol", [(ctc_abi.PREC_FP64, 1e-10), (ctc_abi.PREC_TC, 1e-8)])
+def test_large_explicit_point_call_matches_cubic_grid(torch_cuda, precision, rtol):
+    """Calls of 2^18 points or more pack explicit points sort-tile-recursively
+    (three sorts over the points' bounding box; smaller calls use one Morton
+    sort): the same cube given as explicit points must reproduce the cubic-grid
+    call, and a point sample the oracle."""
+    mol, _ = _cases().CASES["c1"]()
+    m = _mol(mol)
+    origin, axes = _cases().cube_for(mol)
+    shape = (72, 66, 60)  # 285 120 points
+    keys = ("rho", "grad", "lap")
+    cub_ = m.eval_cubic(origin, axes, shape, keys=keys, precision=precision)
+    pts = S.cube_points(origin, axes, shape)
+    assert len(pts) >= 1 << 18
+    got = m.eval_local(pts, keys, precision=precision)
+    idx = np.random.default_rng(3).choice(len(pts), 400, replace=False)
+    ref = O.eval_local(mol.flat(), mol.D, pts[idx], keys=keys)
+    sc = term_scales(mol.flat(), mol.D, pts[idx])
+    for k in keys:
+        g = got[k].reshape(len(pts), -1)
+        c = cub_[k].reshape(len(pts), -1)
+        assert_close(f"{k} oracle", g[idx].reshape(ref[k].shape), ref[k], sc[k], rtol, 1e-14)
+        np.testing.assert_allclose(g, c, rtol=0, atol=rtol * np.abs(c).max())
+
+
 @pytest.mark.parametrize("case", ["esp", "c1", "allshell"])
 def test_esp_vs_oracle(torch_cuda, case):
     mol, pts = _cases().CASES[case]()
