@@ -87,6 +87,14 @@ def test_every_output_slot_and_host_variant(torch_cuda):
     np.testing.assert_allclose(dev["gge"], tf + 0.2 * w + lap / 6, rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(np.trace(dev["hess"], axis1=1, axis2=2), lap, rtol=1e-12, atol=1e-14)
     np.testing.assert_array_equal(dev["hess"], np.transpose(dev["hess"], (0, 2, 1)))
+    # every slot, derived densities included, against the FP64 oracle with the same parameters
+    ref = O.eval_local(mol.flat(), mol.D, pts, alpha=prm[0], keys=tuple(keys), gge_ab=(prm[1], prm[2]),
+                       ked_a=prm[3])
+    sc = term_scales(mol.flat(), mol.D, pts, alpha=prm[0], gge=(prm[1], prm[2]), ked_a=prm[3], ref=ref)
+    live = ref["rho"] > 1e-10
+    for k in keys:
+        mask = live if k in ("rdg", "shannon", "weizsacker", "thomas_fermi", "gge") else None
+        assert_close(f"{k} vs oracle", dev[k].reshape(ref[k].shape), ref[k], sc[k], 1e-10, 1e-14, mask=mask)
 
 
 def test_subsets_match_full_pass(torch_cuda):

@@ -84,6 +84,12 @@ def test_noalloc_matches_eval_local_on_two_calls(torch_cuda):
         want2 = m.eval_local(pts2, KEYS, ctc_abi.PREC_FP64, params=PARAMS)
         _compare("call 1", mol, pts1, got1, want1)
         _compare("call 2", mol, pts2, got2, want2)
+        # and against the FP64 oracle directly, on a sample of the second call
+        from oracle import oracle as O
+        idx = np.random.default_rng(13).choice(len(pts2), 300, replace=False)
+        ref = O.eval_local(mol.flat(), mol.D, pts2[idx], alpha=PARAMS[0], keys=tuple(KEYS),
+                           gge_ab=(PARAMS[1], PARAMS[2]), ked_a=PARAMS[3])
+        _compare("oracle", mol, pts2[idx], {k: v[idx] for k, v in got2.items()}, ref)
     finally:
         m.close()
 
